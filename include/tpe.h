@@ -1,0 +1,239 @@
+/*
+ * tpe.h — C ABI of libtpe, the sm_100a implementation of the constrained
+ * fractional-Sobolev descent step for repulsive curves (tangent-point energy).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns an
+ * int status (TPE_OK = 0) and never throws, traps or aborts across the
+ * boundary. Host buffers are owned by the caller; the library copies them to
+ * device memory owned by the context and writes only into caller-provided
+ * outputs. Vertices are `double[3*V]` interleaved (x0,y0,z0,x1,...), edges are
+ * `int32_t[2*E]` index pairs — the packing a TypeScript shim produces from
+ * `Vec3[]` / `Edge[]` (src/core/testConfigs.ts:1-2).
+ *
+ * The reference interface each entry point replaces is cited beside it
+ * (paths are relative to the reference repository root).
+ */
+#ifndef TPE_H
+#define TPE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TPE_ABI_VERSION 1
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+    TPE_OK = 0,
+    TPE_ERR_BAD_ARG = 1,          /* null pointer, size mismatch, index out of range */
+    TPE_ERR_CUDA = 2,             /* a CUDA runtime call failed; see tpe_last_error */
+    TPE_ERR_SINGULAR = 3,         /* saddle system singular or non-finite (linsolve.ts:247-276 "singular") */
+    TPE_ERR_NONFINITE_INPUT = 4,  /* non-finite right-hand side (linsolve.ts:333-337) */
+    TPE_ERR_NO_TOPOLOGY = 5,      /* tpe_set_topology has not been called */
+    TPE_ERR_OUT_OF_MEMORY = 6,
+    TPE_ERR_INVALID_SET = 7,      /* totalLength + edgeLengths in one set (constraintSet.ts:333-344) */
+    TPE_ERR_REFINE_NOT_CONVERGED = 8, /* mixed path: FP64 refinement hit its cap */
+    TPE_ERR_DEVICE_TIMEOUT = 9,   /* a bounded device-side wait gave up */
+    TPE_ERR_TOO_LARGE = 10        /* request exceeds a fixed-capacity buffer */
+};
+
+/* ---- step outcome reasons (optimizer.ts:186, lineSearch.ts:374-379) ------- */
+enum {
+    TPE_REASON_NONE = 0,
+    TPE_REASON_ZERO_OR_NONFINITE_GRADIENT_NORM = 1,
+    TPE_REASON_NOT_A_DESCENT_DIRECTION = 2,
+    TPE_REASON_ARMIJO_FAILED = 3,
+    TPE_REASON_PROJECTION_FAILED = 4,
+    TPE_REASON_TAU_BELOW_MIN = 5,
+    TPE_REASON_SINGULAR_SYSTEM = 6
+};
+
+/* ---- constraint blocks (constraintSet.ts:39-43 ConstraintBlock) ---------- */
+enum {
+    TPE_BLOCK_BARYCENTER = 0,     /* barycenterBlock(x0)      constraintSet.ts:87-98, 3 rows  */
+    TPE_BLOCK_TOTAL_LENGTH = 1,   /* totalLengthBlock(L0)     constraintSet.ts:119-162, 1 row */
+    TPE_BLOCK_EDGE_LENGTHS = 2,   /* edgeLengthsBlock(ell0)   constraintSet.ts:206-250, E rows */
+    TPE_BLOCK_POINT = 3           /* pointBlock(v, target)    constraintSet.ts:271-301, 3 rows */
+};
+
+/* The plain-data form of one ConstraintBlock: the closure-captured target of
+ * the TypeScript block made explicit so it can cross the FFI. */
+typedef struct {
+    int32_t kind;          /* TPE_BLOCK_* */
+    int32_t vertex;        /* point: pinned vertex (out of range -> NaN rows, as pointBlock) */
+    double target[3];      /* barycenter: x0; point: pin target */
+    double L0;             /* totalLength: frozen L0 (NaN allowed: projection then fails) */
+    const double* ell0;    /* edgeLengths: frozen per-edge targets */
+    int32_t n_ell0;        /* length of ell0; != E -> missing entries are NaN */
+    int32_t reserved;
+} tpe_constraint;
+
+typedef struct {
+    double alpha, beta, epsilon;   /* DEFAULTS = {3, 6, 1e-10} (optimizer.ts:18) */
+} tpe_params;
+
+/* PenaltyConfig (penalties.ts:33-49); weight 0 = off. */
+typedef struct {
+    double total_length;   /* totalLength weight */
+    double length_diff;    /* lengthDiff weight */
+    double field_weight;   /* field.weight */
+    double field_X[3];     /* field.X (normalised inside, |X| < 1e-14 -> off) */
+} tpe_penalties;
+
+enum { TPE_DE_ANALYTICAL = 0, TPE_DE_FINITE_DIFF = 1 };          /* SobolevStepOptions.mode */
+enum { TPE_PROJECTION_REASSEMBLE = 0, TPE_PROJECTION_FROZEN = 1 }; /* ProjectionMode (optimizer.ts:86) */
+enum { TPE_FACTOR_LDLT = 0, TPE_FACTOR_LU = 1 };                  /* FactorMode (linsolve.ts:370) */
+enum { TPE_PRECISION_FP64 = 0, TPE_PRECISION_MIXED = 1 };
+
+/* SobolevStepOptions (optimizer.ts:95-175) + LineSearchOptions (lineSearch.ts:333-371)
+ * + ProjectConstraintSetOptions (lineSearch.ts:120-145), flattened. Fill it with
+ * tpe_default_step_opts() and override fields. */
+typedef struct {
+    int32_t struct_size;           /* sizeof(tpe_step_opts), for versioning */
+    int32_t mode;                  /* TPE_DE_* */
+    double alpha, beta, epsilon, h;
+    int32_t has_energy_before;     /* energyBefore supplied? */
+    int32_t projection_mode;       /* TPE_PROJECTION_* (function default: reassemble) */
+    double energy_before;
+    int32_t factor_mode;           /* TPE_FACTOR_* (accepted; the structured solve ignores it) */
+    int32_t has_penalties;
+    tpe_penalties penalties;
+    double c1, shrink, tau0, tau_min;          /* 1e-4, 0.5, 1, 1e-12 */
+    double proj_tol_abs, proj_tol_rel;         /* 1e-4, 1e-4 */
+    int32_t proj_max_iter;                     /* 8 */
+    int32_t precision;             /* TPE_PRECISION_* (extension) */
+    int32_t trials;                /* tau trials evaluated per batched launch (extension; 1 = sequential) */
+    int32_t collect_field;         /* write g~ into descent_field when non-null */
+    int32_t refine_max_iter;       /* mixed path: FP64 refinement cap (extension) */
+    int32_t reserved;
+    double refine_tol;             /* mixed path: relative residual target (extension) */
+} tpe_step_opts;
+
+/* SobolevStepStats (optimizer.ts:196-202) + LineSearchStepResult (lineSearch.ts:389-400). */
+typedef struct {
+    double energy;                 /* returned objective (energyAfter on accept) */
+    double energy_before;
+    double tau;
+    double residual;               /* saddle relative residual (NaN on singular) */
+    double gradient_l2_norm;       /* ||g~||_{L2h} (NaN on singular) */
+    double slope;                  /* NaN where the reference leaves it undefined */
+    double projection_phi_norm;    /* NaN = null */
+    int32_t accepted;
+    int32_t converged;
+    int32_t projection_iterations; /* -1 = null */
+    int32_t reason;                /* TPE_REASON_* */
+    int32_t refine_iterations;     /* mixed path */
+    int32_t trials_evaluated;      /* tau trials whose energy was evaluated */
+} tpe_step_stats;
+
+/* Phase keys of the timing ledger (phaseTimings.ts:9-20; extra keys appended).
+ * The timings array is double[2*TPE_PHASE_COUNT]: {ms, calls} per key. */
+enum {
+    TPE_PHASE_DE = 0, TPE_PHASE_ENERGY, TPE_PHASE_BHIGH, TPE_PHASE_BLOW, TPE_PHASE_ASSEMBLEA,
+    TPE_PHASE_EXPAND, TPE_PHASE_SADDLE, TPE_PHASE_FACTOR, TPE_PHASE_PROJECTION,
+    TPE_PHASE_LINESEARCH, TPE_PHASE_STEP, TPE_PHASE_REFINE, TPE_PHASE_COUNT
+};
+
+typedef struct tpe_ctx tpe_ctx;
+
+/* ---- context -------------------------------------------------------------- */
+int32_t tpe_abi_version(void);
+void tpe_default_step_opts(tpe_step_opts* opts);
+/* Creates a context bound to CUDA device `device` (one per host thread; the
+ * TypeScript side holds one per Web Worker). Returns NULL on failure with
+ * *status set. */
+tpe_ctx* tpe_create(int32_t device, int32_t* status);
+void tpe_destroy(tpe_ctx* ctx);
+/* Message for the last non-OK status returned on this context. */
+const char* tpe_last_error(const tpe_ctx* ctx);
+
+/* ---- topology ------------------------------------------------------------- */
+/* Replaces calculateDisjointPairs (src/core/tangentPointEnergy.ts:33-47): the
+ * ordered disjoint-pair lists are never materialised; disjointness is tested
+ * in-kernel from endpoint indices. Uploads edges and the vertex->edge
+ * incidence used by the gather kernels. */
+int32_t tpe_set_topology(tpe_ctx* ctx, const int32_t* edges, int32_t E, int32_t V);
+/* Optional: materialise the ordered lists exactly as calculateDisjointPairs
+ * (offsets[E+1], partners[cap]); for callers that still want them. */
+int32_t tpe_disjoint_pairs(tpe_ctx* ctx, int32_t* offsets, int32_t* partners, int64_t cap);
+
+/* ---- energy and its gradient (one FFI energy/gradient entry) -------------- */
+/* calculateEnergy (tangentPointEnergy.ts:50-111). */
+int32_t tpe_energy(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double* energy);
+/* gradientAnalytical (tangentPointEnergy.ts:139-392) fused with the forward
+ * energy; grad may be NULL (energy only) and energy may be NULL. */
+int32_t tpe_energy_grad(tpe_ctx* ctx, const double* xyz, const tpe_params* p,
+                        double* energy, double* grad);
+/* gradientFiniteDiff (tangentPointEnergy.ts:114-136): forward differences. */
+int32_t tpe_gradient_fd(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double h,
+                        double* grad);
+
+/* ---- Gram assembly -------------------------------------------------------- */
+/* assembleBHighFlat / assembleBLowFlat / assembleAFlat (sobolev/innerProduct.ts:38-140,
+ * 177-285, 325-350): V*V row-major outputs, each may be NULL. */
+int32_t tpe_assemble(tpe_ctx* ctx, const double* xyz, const tpe_params* p,
+                     double* B_out, double* B0_out, double* A_out);
+
+/* ---- constraints ---------------------------------------------------------- */
+/* Number of stacked rows k of a set (sum of block row counts). */
+int32_t tpe_constraint_rows(const tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks);
+/* evaluateConstraintSet (sobolev/constraintSet.ts:309-322): phi[k] and the dense
+ * k x 3V Jacobian C (coordinate-block columns, layout.ts:56); C may be NULL. */
+int32_t tpe_evaluate_constraints(tpe_ctx* ctx, const double* xyz, const tpe_constraint* set,
+                                 int32_t nblocks, double* phi, double* C);
+/* l2CurveNorm (sobolev/lineSearch.ts:53-75). */
+int32_t tpe_l2_curve_norm(tpe_ctx* ctx, const double* values, const double* xyz, double* out);
+
+/* ---- saddle solve --------------------------------------------------------- */
+/* solveSaddleFromA (sobolev/linsolve.ts:742-803): solves
+ * [[diag(A,A,A), C^T],[C, 0]] [x; lambda] = [rhs_top; rhs_bottom] with A the
+ * V x V scalar matrix (row-major), C dense k x 3V, rhs_bottom NULL = zeros.
+ * x[3V] coordinate-block layout, lambda[k], residual = ||Kz-rhs||/max(1,||rhs||). */
+int32_t tpe_solve_saddle(tpe_ctx* ctx, const double* A, int32_t n, const double* C, int32_t k,
+                         const double* rhs_top, const double* rhs_bottom, int32_t factor_mode,
+                         double* x, double* lambda, double* residual);
+/* solveConstrainedGradientSet (sobolev/gradient.ts:42-65): assembles A and C at
+ * xyz and solves [[A3,C^T],[C,0]][g;l] = [dE;0]. dE and g_tilde are V x 3 interleaved. */
+int32_t tpe_solve_constrained_gradient(tpe_ctx* ctx, const double* xyz, const double* dE,
+                                       const tpe_constraint* set, int32_t nblocks,
+                                       const tpe_step_opts* opts, double* g_tilde,
+                                       double* lambda, double* residual);
+
+/* ---- projection, line search, the step ------------------------------------ */
+/* projectOntoConstraintSet (sobolev/lineSearch.ts:196-295). base_xyz != NULL
+ * selects the frozen operator K(base) (solveConstrainedGradientSetFrozen's
+ * operator); NULL reassembles at every iterate. */
+int32_t tpe_project(tpe_ctx* ctx, const double* xyz, const tpe_constraint* set, int32_t nblocks,
+                    const tpe_step_opts* opts, const double* base_xyz, double* xyz_out,
+                    int32_t* ok, int32_t* iterations, double* phi_norm);
+/* lineSearchStepSet (sobolev/lineSearch.ts:423-562), dE / g_tilde supplied by
+ * the caller; opts->projection_mode FROZEN freezes K at xyz. */
+int32_t tpe_line_search_step(tpe_ctx* ctx, const double* xyz, const double* dE,
+                             const double* g_tilde, const tpe_constraint* set, int32_t nblocks,
+                             const tpe_step_opts* opts, double* xyz_out, tpe_step_stats* stats);
+/* sobolevStepSet (src/core/optimizer.ts:231-440): the whole step. timings is
+ * double[2*TPE_PHASE_COUNT] or NULL; descent_field (V x 3) receives g~ when
+ * opts->collect_field and non-NULL. */
+int32_t tpe_sobolev_step(tpe_ctx* ctx, const double* xyz, const tpe_constraint* set,
+                         int32_t nblocks, const tpe_step_opts* opts, double* xyz_out,
+                         tpe_step_stats* stats, double* timings, double* descent_field);
+
+/* ---- penalties (sobolev/penalties.ts:139-241) ----------------------------- */
+int32_t tpe_penalty_energy(tpe_ctx* ctx, const double* xyz, const tpe_penalties* pen,
+                           double* energy);
+int32_t tpe_penalty_gradient(tpe_ctx* ctx, const double* xyz, const tpe_penalties* pen,
+                             double* grad);
+
+/* ---- batching (no single reference counterpart: many sobolevStepSet calls) */
+/* Energies of `ncurves` curves that share this context's topology (e.g. the K
+ * tau-trial candidates of one line search) in one launch: xyz is
+ * ncurves x V x 3, energies[ncurves]. */
+int32_t tpe_energy_batch(tpe_ctx* ctx, const double* xyz, int32_t ncurves, const tpe_params* p,
+                         int32_t precision, double* energies);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TPE_H */
