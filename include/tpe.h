@@ -233,6 +233,26 @@ int32_t tpe_penalty_gradient(tpe_ctx* ctx, const double* xyz, const tpe_penaltie
 int32_t tpe_energy_batch(tpe_ctx* ctx, const double* xyz, int32_t ncurves, const tpe_params* p,
                          int32_t precision, double* energies);
 
+/* ---- device-resident step and instrumentation (extensions) ------------------ */
+/* sobolevStepSet with the vertices already in device memory (d_xyz, d_xyz_out
+ * are V x 3 device pointers on this context's device); for callers that keep
+ * the curve resident between steps. Same semantics as tpe_sobolev_step. */
+int32_t tpe_sobolev_step_device(tpe_ctx* ctx, const double* d_xyz, const tpe_constraint* set,
+                                int32_t nblocks, const tpe_step_opts* opts, double* d_xyz_out,
+                                tpe_step_stats* stats, double* timings);
+/* The CUDA stream (cudaStream_t) every launch of this context is issued on. */
+void* tpe_stream(tpe_ctx* ctx);
+/* Kernel groups timed with CUDA events on that stream while profiling is on. */
+enum {
+    TPE_KGROUP_ENERGY = 0, TPE_KGROUP_GRADIENT, TPE_KGROUP_PAIR_WEIGHTS, TPE_KGROUP_GATHER_A,
+    TPE_KGROUP_CHOLESKY, TPE_KGROUP_TRSV, TPE_KGROUP_OTHER, TPE_KGROUP_COUNT
+};
+/* on != 0 resets and starts event timing; 0 stops it. */
+int32_t tpe_profile(tpe_ctx* ctx, int32_t on);
+/* Per group: total milliseconds and kernel launches since tpe_profile(ctx, 1);
+ * launches[TPE_KGROUP_COUNT] also counts every kernel this context launched. */
+int32_t tpe_profile_read(tpe_ctx* ctx, double* ms, int64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,185 @@
+// Internal declarations of libtpe: the context, device buffers and the
+// launchers each .cu file provides. Not part of the ABI (include/tpe.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tpe.h"
+
+#define TPE_CUDA_TRY(expr)                                                              \
+    do {                                                                                \
+        cudaError_t _e = (expr);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            tpe::set_error(ctx, TPE_ERR_CUDA, std::string(#expr) + ": " +               \
+                                                  cudaGetErrorString(_e));              \
+            return TPE_ERR_CUDA;                                                        \
+        }                                                                               \
+    } while (0)
+
+#define TPE_TRY(expr)                       \
+    do {                                    \
+        int32_t _s = (expr);                \
+        if (_s != TPE_OK) return _s;        \
+    } while (0)
+
+namespace tpe {
+
+// A grow-only device allocation owned by the context.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Dense Cholesky block size (diagonal blocks are factored by one CTA).
+constexpr int kNB = 64;
+
+// Everything the structured saddle solve keeps between the factorization and
+// later solves: the frozen operator of optimizer.ts's 'frozen' projection.
+struct SaddleOp {
+    bool valid = false;
+    int V = 0, k = 0;
+    bool trans_constrained = false;  // set contains a barycenter or point block
+    double rho = 0.0;                // A_rho = A + (rho/V) 1 1^T
+    // device (views into ctx buffers)
+    double* A = nullptr;     // V x V original A (unfactored, for residuals)
+    double* L = nullptr;     // V x V Cholesky factor of A_rho (lower, row-major)
+    double* Linv = nullptr;  // nb x 64 x 64 inverses of the diagonal blocks of L
+    double* C = nullptr;     // k x 3V dense constraint Jacobian
+    double* Y = nullptr;     // k x 3V: Abar_rho^{-1} C^T (row s = column s of C^T)
+    // host: small Schur complement and its factors
+    std::vector<double> Scc;   // k x k, then its Cholesky factor (lower)
+    std::vector<double> Scu;   // k x 3 = C U / rho
+    std::vector<double> M;     // 3 x 3 = Scu^T Scc^{-1} Scu, then its Cholesky factor
+};
+
+struct DevBlock {
+    int32_t kind;
+    int32_t row0;
+    int32_t vertex;
+    int32_t rows;
+    double target[3];
+    double L0;
+    const double* ell0;  // device copy, E entries (NaN where the host array ended)
+};
+
+}  // namespace tpe
+
+struct tpe_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int32_t num_sms = 0;
+
+    // topology
+    bool has_topology = false;
+    int32_t V = 0, E = 0;
+    std::vector<int32_t> h_edges;     // 2E
+    std::vector<int32_t> h_inc_off;   // V+1
+    std::vector<int32_t> h_inc;       // 2E entries: edge*2 + slot, ascending edge order per vertex
+    tpe::DevBuf d_edges, d_inc_off, d_inc;
+
+    // per-evaluation buffers
+    tpe::DevBuf pos, pos2, pos3, edge_a, edge_b, grad, edge_acc, partial, scalars, flat0, flat1,
+        flat2, flat3, dir;
+    tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
+    tpe::DevBuf mat_A, mat_L, mat_Linv, mat_B, mat_B0;
+    tpe::DevBuf con_C, con_Y, con_phi, con_blocks, con_ell0, con_red;
+    tpe::DevBuf rhs, sol, tmp, solve_scratch;
+    tpe::DevBuf status;                     // device-side int flags
+    tpe::SaddleOp op;
+    std::vector<double> h_tmp;
+
+    // instrumentation: kernel launch count and per-group CUDA-event timing
+    int64_t launches = 0;
+    bool profiling = false;
+    double prof_ms[TPE_KGROUP_COUNT] = {};
+    int64_t prof_launches[TPE_KGROUP_COUNT + 1] = {};
+    struct PendingEvent {
+        int group;
+        cudaEvent_t a, b;
+    };
+    std::vector<PendingEvent> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+};
+
+namespace tpe {
+
+// Times the launches issued while in scope under `group` (when profiling) and
+// counts them; `n` = number of kernels the scope launches.
+struct KernelScope {
+    tpe_ctx* ctx;
+    int group;
+    cudaEvent_t b = nullptr;
+    KernelScope(tpe_ctx* c, int g, int64_t n);
+    ~KernelScope();
+};
+
+void set_error(tpe_ctx* ctx, int32_t code, const std::string& msg);
+int32_t ensure(tpe_ctx* ctx, DevBuf& b, size_t bytes);
+
+// ---- pair kernels (pair_kernels.cu) ----------------------------------------
+// Per-edge records from interleaved positions: a = (p1, ell^eps), b = (p2, |e|).
+int32_t edge_prep(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps,
+                  double alpha);
+// Energy of ncurves position sets (edge records already prepared) into
+// d_energy[ncurves] (device).
+int32_t energy_fp64(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, double eps,
+                    double* d_energy);
+// Energy (optional) and gradient (interleaved V x 3) of one curve.
+int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
+                         double* d_grad);
+
+// ---- assembly (assembly.cu) -----------------------------------------------
+// A (and optionally B, B0) V x V row-major FP64 from prepared edge records.
+int32_t assemble_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_A,
+                      double* d_B, double* d_B0);
+
+// ---- dense linear algebra (dense.cu) --------------------------------------
+// In-place lower Cholesky of the V x V row-major matrix (lower triangle read);
+// also writes the inverses of the 64x64 diagonal blocks. Sets *singular.
+int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, double piv_tol,
+                      int32_t* singular);
+// Solves (L L^T) X = B in place for nrhs right-hand sides stored as B[nrhs][n].
+int32_t chol_solve_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
+                        double* d_B, int32_t nrhs);
+// out[i*ncols + j] = dot(X[i], Y[j]) over len (rows of length len): FP64, deterministic.
+int32_t gram_dots(tpe_ctx* ctx, const double* X, int32_t nx, const double* Y, int32_t ny,
+                  int64_t len, double* d_out);
+// A_rho = A + shift (every entry) into L (lower triangle copied), and trace(A) into *d_trace.
+int32_t shift_copy(tpe_ctx* ctx, const double* d_A, double* d_L, int32_t n, double shift);
+int32_t trace(tpe_ctx* ctx, const double* d_A, int32_t n, double* d_out);
+
+// ---- constraints (constraints.cu) -----------------------------------------
+// Upload the set, returns k (stacked rows).
+int32_t upload_set(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, int32_t* k);
+// Phi (k) and per-block {norm^2, scale} (2*nblocks) into host arrays; dense C
+// (k x 3V, device) when d_C != nullptr.
+int32_t eval_constraints(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k,
+                         double* d_C, std::vector<double>& phi, std::vector<double>& norm_scale);
+
+// ---- small device helpers (dense.cu) --------------------------------------
+int32_t interleaved_to_block(tpe_ctx* ctx, const double* d_v3, double* d_flat, int32_t V);
+int32_t block_to_interleaved(tpe_ctx* ctx, const double* d_flat, double* d_v3, int32_t V);
+// y = a*x + b*y (n)
+int32_t axpby(tpe_ctx* ctx, int64_t n, double a, const double* x, double b, double* y);
+// host result: sum(x*y) over n (deterministic)
+int32_t dot(tpe_ctx* ctx, int64_t n, const double* x, const double* y, double* out);
+// host result: number of non-finite entries in x[n]
+int32_t count_nonfinite(tpe_ctx* ctx, int64_t n, const double* x, int64_t* out);
+// l2CurveNorm of interleaved values at interleaved positions (host result)
+int32_t l2_curve_norm(tpe_ctx* ctx, const double* d_vals, const double* d_pos, double* out);
+// x_flat(3V) = w - sum_s Y[s] * lam[s] - U mu / rho ; lam/mu are host arrays
+int32_t combine_solution(tpe_ctx* ctx, const double* d_w, const double* d_Y, int32_t k,
+                         const double* lam, const double* mu, double rho, int32_t V, double* d_x);
+// Structured residual ||K z - rhs|| / max(1, ||rhs||) with A (V x V), C (k x 3V).
+int32_t saddle_residual(tpe_ctx* ctx, const double* d_A, int32_t V, const double* d_C, int32_t k,
+                        const double* d_x, const double* lam, const double* d_rhs_top,
+                        const double* rhs_bottom, double* out);
+
+}  // namespace tpe
