@@ -290,13 +290,16 @@ int32_t check_topology(tpe_ctx* ctx) {
 
 // Factor A_rho and the Schur complement from ctx->mat_A (V x V) and ctx->con_C (k x 3V).
 // *singular set when the reference would report a singular system.
-int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular) {
+int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
+                    const double* b_flat = nullptr) {
     SaddleOp& op = ctx->op;
     op.valid = false;
     op.V = V;
     op.k = k;
     op.A = ctx->mat_A.as<double>();
     op.C = ctx->con_C.as<double>();
+    op.W = nullptr;
+    op.w_src = nullptr;
     *singular = false;
     const int32_t nb = (V + kNB - 1) / kNB;
     TPE_TRY(ensure(ctx, ctx->mat_L, sizeof(double) * (size_t)V * V));
@@ -338,16 +341,27 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular) {
     op.Scc.assign((size_t)k * k, 0.0);
     op.Scu.assign((size_t)k * 3, 0.0);
     op.trans_constrained = false;
-    if (k > 0) {
-        TPE_TRY(ensure(ctx, ctx->con_Y, sizeof(double) * (size_t)k * 3 * V));
+    // One triangular solve for Y = Abar_rho^{-1} C^T (3k right-hand sides of
+    // length V) and, when given, w = Abar_rho^{-1} b (3 more), in groups of 64.
+    {
+        const int32_t rows = k + (b_flat ? 1 : 0);
+        TPE_TRY(ensure(ctx, ctx->con_Y, sizeof(double) * (size_t)(rows > 0 ? rows : 1) * 3 * V));
         op.Y = ctx->con_Y.as<double>();
-        TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
-        // 3k right-hand sides of length V, in groups of at most 64
-        for (int32_t r0 = 0; r0 < 3 * k; r0 += 64) {
-            const int32_t nr = (3 * k - r0) < 64 ? (3 * k - r0) : 64;
+        if (k > 0)
+            TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+        if (b_flat) {
+            op.W = op.Y + (size_t)k * 3 * V;
+            op.w_src = b_flat;
+            TPE_CUDA_TRY(cudaMemcpyAsync(op.W, b_flat, sizeof(double) * 3 * (size_t)V,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        for (int32_t r0 = 0; r0 < 3 * rows; r0 += 64) {
+            const int32_t nr = (3 * rows - r0) < 64 ? (3 * rows - r0) : 64;
             TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, op.Y + (size_t)r0 * V, nr));
         }
+    }
+    if (k > 0) {
         TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * ((size_t)k * k + 4 * (size_t)k + 16)));
         double* dS = ctx->tmp.as<double>();
         TPE_TRY(gram_dots(ctx, op.C, k, op.Y, k, 3 * (int64_t)V, dS));
@@ -413,7 +427,8 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular) {
 
 // Assemble A and C at device positions d_pos (set already uploaded) and factor.
 int32_t op_build(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k, double alpha,
-                 double beta, double eps, bool* singular, double* timings) {
+                 double beta, double eps, bool* singular, double* timings,
+                 const double* b_flat = nullptr) {
     const int32_t V = ctx->V;
     {
         Timer t(ctx, timings, TPE_PHASE_ASSEMBLEA);
@@ -425,7 +440,7 @@ int32_t op_build(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k, 
     std::vector<double> phi, ns;
     TPE_TRY(eval_constraints(ctx, d_pos, nblocks, k, ctx->con_C.as<double>(), phi, ns));
     Timer t(ctx, timings, TPE_PHASE_FACTOR);
-    return op_finalize(ctx, V, k, singular);
+    return op_finalize(ctx, V, k, singular, b_flat);
 }
 
 // Solve with the current operator: b_flat (device, 3V, or null = 0), d (host, k,
@@ -439,9 +454,13 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
     double* w = ctx->flat0.as<double>();
     std::vector<double> rc((size_t)k, 0.0), ru(3, 0.0);
     if (b_flat) {
-        TPE_CUDA_TRY(cudaMemcpyAsync(w, b_flat, sizeof(double) * m, cudaMemcpyDeviceToDevice,
-                                     ctx->stream));
-        TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, w, 3));
+        if (op.W && op.w_src == b_flat) {
+            w = op.W;  // solved together with Y at factor time
+        } else {
+            TPE_CUDA_TRY(cudaMemcpyAsync(w, b_flat, sizeof(double) * m, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+            TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, w, 3));
+        }
         if (k > 0) {
             TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * ((size_t)k + 16)));
             TPE_TRY(gram_dots(ctx, op.C, k, w, 1, m, ctx->tmp.as<double>()));
@@ -486,8 +505,9 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
     if (residual) {
         const double* top = b_flat;
         if (!top) {
-            TPE_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(double) * m, ctx->stream));
-            top = w;
+            double* z = ctx->flat0.as<double>();
+            TPE_CUDA_TRY(cudaMemsetAsync(z, 0, sizeof(double) * m, ctx->stream));
+            top = z;
         }
         std::vector<double> bottom((size_t)k, 0.0);
         if (d)
@@ -1009,7 +1029,7 @@ int32_t tpe_solve_saddle(tpe_ctx* ctx, const double* A, int32_t n, const double*
     if (k > 0) TPE_TRY(upload(ctx, ctx->con_C, C, sizeof(double) * (size_t)k * m));
     TPE_TRY(upload(ctx, ctx->flat2, rhs_top, sizeof(double) * m));
     bool singular = false;
-    TPE_TRY(op_finalize(ctx, n, k, &singular));
+    TPE_TRY(op_finalize(ctx, n, k, &singular, ctx->flat2.as<double>()));
     if (singular) {
         set_error(ctx, TPE_ERR_SINGULAR, "saddle system is singular");
         return TPE_ERR_SINGULAR;
@@ -1037,16 +1057,16 @@ int32_t tpe_solve_constrained_gradient(tpe_ctx* ctx, const double* xyz, const do
     TPE_TRY(set_k(ctx, set, nblocks, &S));
     TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
     TPE_TRY(upload(ctx, ctx->grad, dE, sizeof(double) * m));
+    TPE_TRY(ensure(ctx, ctx->flat2, sizeof(double) * m));
+    TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
+    TPE_TRY(interleaved_to_block(ctx, ctx->grad.as<double>(), ctx->flat2.as<double>(), V));
     bool singular = false;
     TPE_TRY(op_build(ctx, ctx->pos.as<double>(), nblocks, S.k, o->alpha, o->beta, o->epsilon,
-                     &singular, nullptr));
+                     &singular, nullptr, ctx->flat2.as<double>()));
     if (singular) {
         set_error(ctx, TPE_ERR_SINGULAR, "saddle system is singular");
         return TPE_ERR_SINGULAR;
     }
-    TPE_TRY(ensure(ctx, ctx->flat2, sizeof(double) * m));
-    TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
-    TPE_TRY(interleaved_to_block(ctx, ctx->grad.as<double>(), ctx->flat2.as<double>(), V));
     std::vector<double> lam;
     double res = 0.0;
     TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), nullptr, ctx->flat1.as<double>(), lam, &res));
@@ -1148,8 +1168,11 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
         }
     }
     if (pen) TPE_TRY(penalty_gradient_dev(ctx, P, &o->penalties, dE, 1));
+    TPE_TRY(ensure(ctx, ctx->flat2, sizeof(double) * m));
+    TPE_TRY(interleaved_to_block(ctx, dE, ctx->flat2.as<double>(), V));
     bool singular = false;
-    TPE_TRY(op_build(ctx, P, nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular, timings));
+    TPE_TRY(op_build(ctx, P, nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular, timings,
+                     ctx->flat2.as<double>()));
     TPE_TRY(ensure(ctx, ctx->sol, sizeof(double) * m));
     double* out = ctx->sol.as<double>();
     if (singular) {
@@ -1159,10 +1182,8 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
         st->reason = TPE_REASON_SINGULAR_SYSTEM;
         return TPE_OK;
     }
-    TPE_TRY(ensure(ctx, ctx->flat2, sizeof(double) * m));
     TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
     TPE_TRY(ensure(ctx, ctx->rhs, sizeof(double) * m));
-    TPE_TRY(interleaved_to_block(ctx, dE, ctx->flat2.as<double>(), V));
     std::vector<double> lam;
     double res = 0.0;
     {

@@ -24,8 +24,6 @@
 namespace tpe {
 namespace {
 
-constexpr int kThreads = 128;
-constexpr int kTile = 128;
 
 __device__ __forceinline__ bool disjoint(int2 a, int2 b) {
     return a.x != b.x && a.x != b.y && a.y != b.x && a.y != b.y;
@@ -38,94 +36,158 @@ __device__ __forceinline__ double inv_dist_pow(double dn, double distExp) {
     return 1.0 / pow(dn, distExp);
 }
 
+constexpr int kT = 32;  // pair tile: 32 edges I x 32 edges J
+
+struct EdgeRec {
+    double4 p1;  // endpoint 1, l^eps
+    double4 p2;  // endpoint 2
+    double4 T;   // unit tangent (0 below 1e-14), raw length
+    int2 ij;
+};
+
+__device__ __forceinline__ void load_edge(const double4* __restrict__ ea,
+                                          const double4* __restrict__ eb,
+                                          const int2* __restrict__ edges, int32_t E, int32_t I,
+                                          EdgeRec& r) {
+    if (I >= E) {
+        r.p1 = make_double4(0, 0, 0, 1);
+        r.p2 = make_double4(0, 0, 0, 1);
+        r.T = make_double4(0, 0, 0, 0);
+        r.ij = make_int2(-1, -1);
+        return;
+    }
+    r.p1 = ea[I];
+    r.p2 = eb[I];
+    r.ij = edges[I];
+    const double ex = r.p2.x - r.p1.x, ey = r.p2.y - r.p1.y, ez = r.p2.z - r.p1.z;
+    const double len = sqrt(ex * ex + ey * ey + ez * ez);
+    if (len < 1e-14) {
+        r.T = make_double4(0, 0, 0, len);
+    } else {
+        const double inv = 1.0 / len;
+        r.T = make_double4(ex * inv, ey * inv, ez * inv, len);
+    }
+}
+
+// Symmetric pair weights of one unordered pair: (w_IJ + w_JI, q_IJ + q_JI).
 template <int MODE>
-__global__ void __launch_bounds__(kThreads)
+__device__ __forceinline__ double2 pair_weight(const EdgeRec& a, const EdgeRec& b, double distExp,
+                                               double eps) {
+    double sumDist = 0.0, sumLowIJ = 0.0, sumLowJI = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        const int ai = s >> 1, bj = s & 1;
+        const double dx = (ai ? a.p2.x : a.p1.x) - (bj ? b.p2.x : b.p1.x);
+        const double dy = (ai ? a.p2.y : a.p1.y) - (bj ? b.p2.y : b.p1.y);
+        const double dz = (ai ? a.p2.z : a.p1.z) - (bj ? b.p2.z : b.p1.z);
+        const double dn = sqrt(dx * dx + dy * dy + dz * dz) + eps;
+        const double kd = inv_dist_pow<MODE>(dn, distExp);
+        sumDist += kd;
+        const double dn2 = dn * dn;
+        const double kq = kd / (dn2 * dn2);
+        double cx = a.T.y * dz - a.T.z * dy, cy = a.T.z * dx - a.T.x * dz,
+               cz = a.T.x * dy - a.T.y * dx;
+        double cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
+        sumLowIJ += cn * cn * kq;
+        cx = b.T.y * dz - b.T.z * dy;
+        cy = b.T.z * dx - b.T.x * dz;
+        cz = b.T.x * dy - b.T.y * dx;
+        cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
+        sumLowJI += cn * cn * kq;
+    }
+    const double ll = a.p1.w * b.p1.w;
+    return make_double2(0.5 * ll * sumDist, 0.0625 * ll * (sumLowIJ + sumLowJI));
+}
+
+// One block per upper-triangular 32x32 tile (it <= jt) of the E x E pair
+// matrix; 256 threads = 32 J lanes x 8 row groups of 4 I rows. Writes
+// M[I][J] = (-(w_IJ+w_JI) T_I.T_J / (l_I l_J), -(q_IJ+q_JI)) coalesced along J,
+// and its mirror M[J][I] through a shared-memory transpose. Row sums of the
+// weights go to rowpart[slot][row] (slot = the other tile index), each slot
+// written once, for the diagonal pass.
+template <int MODE>
+__global__ void __launch_bounds__(256)
 pair_weights_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
                     const int2* __restrict__ edges, int32_t E, double distExp, double eps,
-                    double2* __restrict__ M) {
-    __shared__ double4 sa[kTile], sb[kTile];
-    __shared__ int2 se[kTile];
-    const int32_t I = blockIdx.x * kThreads + threadIdx.x;
-    const bool valid = I < E;
-    double4 a = make_double4(0, 0, 0, 1), b = make_double4(0, 0, 0, 1);
-    int2 ei = make_int2(-1, -1);
-    if (valid) {
-        a = ea[I];
-        b = eb[I];
-        ei = edges[I];
-    }
-    const double eIx = b.x - a.x, eIy = b.y - a.y, eIz = b.z - a.z;
-    const double rI = sqrt(eIx * eIx + eIy * eIy + eIz * eIz);
-    double TIx = 0, TIy = 0, TIz = 0;
-    if (!(rI < 1e-14)) {
-        const double inv = 1.0 / rI;
-        TIx = eIx * inv;
-        TIy = eIy * inv;
-        TIz = eIz * inv;
-    }
-    const double ellI = a.w;
-    double dsum = 0.0, d0sum = 0.0;
-    double2* row = M + (int64_t)I * E;
-    for (int32_t t0 = 0; t0 < E; t0 += kTile) {
-        const int32_t nt = min(kTile, E - t0);
-        __syncthreads();
-        if (threadIdx.x < nt) {
-            sa[threadIdx.x] = ea[t0 + threadIdx.x];
-            sb[threadIdx.x] = eb[t0 + threadIdx.x];
-            se[threadIdx.x] = edges[t0 + threadIdx.x];
-        }
-        __syncthreads();
-        if (!valid) continue;
-        for (int32_t jj = 0; jj < nt; jj++) {
-            const int32_t J = t0 + jj;
-            const int2 ej = se[jj];
-            double2 out = make_double2(0.0, 0.0);
-            if (J != I && disjoint(ei, ej)) {
-                const double4 qa = sa[jj], qb = sb[jj];
-                const double eJx = qb.x - qa.x, eJy = qb.y - qa.y, eJz = qb.z - qa.z;
-                const double rJ = sqrt(eJx * eJx + eJy * eJy + eJz * eJz);
-                double TJx = 0, TJy = 0, TJz = 0;
-                if (!(rJ < 1e-14)) {
-                    const double inv = 1.0 / rJ;
-                    TJx = eJx * inv;
-                    TJy = eJy * inv;
-                    TJz = eJz * inv;
-                }
-                const double ellJ = qa.w;
-                double sumDist = 0.0, sumLowIJ = 0.0, sumLowJI = 0.0;
+                    double2* __restrict__ M, double2* __restrict__ rowpart) {
+    __shared__ EdgeRec sI[kT], sJ[kT];
+    __shared__ double2 tile[kT][kT + 1];
+    __shared__ double2 colred[8][kT];
+    const int64_t t = blockIdx.x;
+    int32_t it = (int32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((int64_t)it * (it + 1) / 2 > t) it--;
+    while ((int64_t)(it + 1) * (it + 2) / 2 <= t) it++;
+    const int32_t jt_rel = (int32_t)(t - (int64_t)it * (it + 1) / 2);
+    // map the lower-triangle enumeration (it >= jt_rel) to the upper tile (row jt_rel, col it)
+    const int32_t ti = jt_rel, tj = it;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    if (threadIdx.x < kT) load_edge(ea, eb, edges, E, ti * kT + threadIdx.x, sI[threadIdx.x]);
+    else if (threadIdx.x < 2 * kT)
+        load_edge(ea, eb, edges, E, tj * kT + threadIdx.x - kT, sJ[threadIdx.x - kT]);
+    __syncthreads();
+    const int32_t J = tj * kT + tx;
+    const EdgeRec& b = sJ[tx];
+    double2 colsum = make_double2(0.0, 0.0);
 #pragma unroll
-                for (int s = 0; s < 4; s++) {
-                    const int ai = s >> 1, bj = s & 1;
-                    const double dx = (ai ? b.x : a.x) - (bj ? qb.x : qa.x);
-                    const double dy = (ai ? b.y : a.y) - (bj ? qb.y : qa.y);
-                    const double dz = (ai ? b.z : a.z) - (bj ? qb.z : qa.z);
-                    const double dn = sqrt(dx * dx + dy * dy + dz * dz) + eps;
-                    const double kd = inv_dist_pow<MODE>(dn, distExp);
-                    sumDist += kd;
-                    const double dn2 = dn * dn;
-                    const double kq = kd / (dn2 * dn2);
-                    double cx = TIy * dz - TIz * dy, cy = TIz * dx - TIx * dz,
-                           cz = TIx * dy - TIy * dx;
-                    double cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
-                    sumLowIJ += cn * cn * kq;
-                    cx = TJy * dz - TJz * dy;
-                    cy = TJz * dx - TJx * dz;
-                    cz = TJx * dy - TJy * dx;
-                    cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
-                    sumLowJI += cn * cn * kq;
-                }
-                const double ll = ellI * ellJ;
-                const double w2 = 0.5 * ll * sumDist;             // w_IJ + w_JI
-                const double q = 0.0625 * ll * (sumLowIJ + sumLowJI);  // q_IJ + q_JI
-                const double dotT = TIx * TJx + TIy * TJy + TIz * TJz;
-                dsum += w2;
-                d0sum += q;
-                out = make_double2(-w2 * dotT / ll, -q);
-            }
-            row[J] = out;
+    for (int r = 0; r < 4; r++) {
+        const int li = ty + 8 * r;
+        const int32_t I = ti * kT + li;
+        const EdgeRec& a = sI[li];
+        double2 out = make_double2(0.0, 0.0);
+        double2 w = make_double2(0.0, 0.0);
+        const bool ok = I < E && J < E && I != J && a.ij.x != b.ij.x && a.ij.x != b.ij.y &&
+                        a.ij.y != b.ij.x && a.ij.y != b.ij.y;
+        if (ok) {
+            w = pair_weight<MODE>(a, b, distExp, eps);
+            const double dotT = a.T.x * b.T.x + a.T.y * b.T.y + a.T.z * b.T.z;
+            out = make_double2(-w.x * dotT / (a.p1.w * b.p1.w), -w.y);
         }
+        if (I < E && J < E) M[(int64_t)I * E + J] = out;
+        tile[li][tx] = out;
+        colsum.x += w.x;
+        colsum.y += w.y;
+        // row sum over this tile's J (warp = one row group)
+        double2 rs = w;
+        for (int o = 16; o > 0; o >>= 1) {
+            rs.x += __shfl_down_sync(0xffffffffu, rs.x, o);
+            rs.y += __shfl_down_sync(0xffffffffu, rs.y, o);
+        }
+        if (tx == 0 && I < E) rowpart[(int64_t)tj * E + I] = rs;
     }
-    if (valid) row[I] = make_double2(dsum / (ellI * ellI), d0sum);
+    if (ti == tj) return;  // diagonal tile: every (I, J) was computed directly
+    colred[ty][tx] = colsum;
+    __syncthreads();
+    // mirror: M[J][I] for I in tile ti, written along I
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int lj = ty + 8 * r;
+        const int32_t Jr = tj * kT + lj;
+        const int32_t Ic = ti * kT + tx;
+        if (Jr < E && Ic < E) M[(int64_t)Jr * E + Ic] = tile[tx][lj];
+    }
+    if (ty == 0 && J < E) {
+        double2 s = colred[0][tx];
+        for (int g = 1; g < 8; g++) {
+            s.x += colred[g][tx].x;
+            s.y += colred[g][tx].y;
+        }
+        rowpart[(int64_t)ti * E + J] = s;
+    }
+}
+
+// Diagonal of the pair matrix: (d_I, d0_I) from the per-tile row sums.
+__global__ void pair_diag_kernel(const double4* __restrict__ ea, int32_t E, int32_t nt,
+                                 const double2* __restrict__ rowpart, double2* __restrict__ M) {
+    const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= E) return;
+    double sx = 0.0, sy = 0.0;
+    for (int32_t s = 0; s < nt; s++) {
+        const double2 p = rowpart[(int64_t)s * E + I];
+        sx += p.x;
+        sy += p.y;
+    }
+    const double ell = ea[I].w;
+    M[(int64_t)I * E + I] = make_double2(sx / (ell * ell), sy);
 }
 
 // A[v][u] = sum_{(I,a) in inc(v)} sum_{(J,b) in inc(u)} (s_a s_b Mb'[I][J] + M0'[I][J]),
@@ -182,18 +244,22 @@ int32_t assemble_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, doubl
     const double sigma = s - 1.0;
     const double distExp = 2.0 * sigma + 1.0;
     const int mode = (alpha == 3.0 && beta == 6.0) ? 1 : 0;
-    const int32_t xb = (E + kThreads - 1) / kThreads;
+    const int32_t ntp = (E + kT - 1) / kT;
+    TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double2) * (size_t)ntp * E));
     {
-    KernelScope ks(ctx, TPE_KGROUP_PAIR_WEIGHTS, 1);
-    if (mode == 1)
-        pair_weights_kernel<1><<<xb, kThreads, 0, ctx->stream>>>(
-            ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
-            distExp, eps, ctx->pairM.as<double2>());
-    else
-        pair_weights_kernel<0><<<xb, kThreads, 0, ctx->stream>>>(
-            ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
-            distExp, eps, ctx->pairM.as<double2>());
-    TPE_CUDA_TRY(cudaGetLastError());
+        KernelScope ks(ctx, TPE_KGROUP_PAIR_WEIGHTS, 2);
+        const int64_t tiles = (int64_t)ntp * (ntp + 1) / 2;
+        if (mode == 1)
+            pair_weights_kernel<1><<<(unsigned)tiles, 256, 0, ctx->stream>>>(
+                ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
+                distExp, eps, ctx->pairM.as<double2>(), ctx->tmp.as<double2>());
+        else
+            pair_weights_kernel<0><<<(unsigned)tiles, 256, 0, ctx->stream>>>(
+                ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
+                distExp, eps, ctx->pairM.as<double2>(), ctx->tmp.as<double2>());
+        pair_diag_kernel<<<(E + 255) / 256, 256, 0, ctx->stream>>>(
+            ctx->edge_a.as<double4>(), E, ntp, ctx->tmp.as<double2>(), ctx->pairM.as<double2>());
+        TPE_CUDA_TRY(cudaGetLastError());
     }
     const int32_t nt = (V + 31) / 32;
     KernelScope ks(ctx, TPE_KGROUP_GATHER_A, 1);

@@ -126,126 +126,171 @@ trsm_panel_kernel(double* __restrict__ L, const double* __restrict__ Linv, int32
     }
 }
 
-// Trailing update: A_ij -= L_ik L_jk^T for kb < jb <= ib (lower triangle).
+// Trailing update A_ij -= L_ik L_jk^T over the lower triangle of the trailing
+// matrix, in 128 x 128 tiles (rank-64 update, K = the panel). 256 threads, each
+// an 8 x 8 register tile; the two 128 x 64 panels are staged transposed in
+// shared memory; a thread owns rows 8ty..8ty+7 and columns 2tx + 32q + {0,1}.
+constexpr int ST = 128;
+constexpr int SP = ST + 2;
 __global__ void __launch_bounds__(256)
 syrk_update_kernel(double* __restrict__ L, int32_t n, int32_t kb) {
     extern __shared__ double dsm[];
-    double(*at)[NB + 2] = reinterpret_cast<double(*)[NB + 2]>(dsm);                  // at[m][r] = L_ik[r][m]
-    double(*bt)[NB + 2] = reinterpret_cast<double(*)[NB + 2]>(dsm + NB * (NB + 2));  // bt[m][c] = L_jk[c][m]
+    double* at = dsm;            // at[m * SP + r] = L[r0 + r][k0 + m]
+    double* bt = dsm + NB * SP;  // bt[m * SP + c] = L[c0 + c][k0 + m]
     const int64_t t = blockIdx.x;
     int32_t ti = (int32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
     while ((int64_t)ti * (ti + 1) / 2 > t) ti--;
     while ((int64_t)(ti + 1) * (ti + 2) / 2 <= t) ti++;
     const int32_t tj = (int32_t)(t - (int64_t)ti * (ti + 1) / 2);
-    const int32_t ib = kb + 1 + ti, jb = kb + 1 + tj;
-    const int32_t r0 = ib * NB, cc0 = jb * NB, k0 = kb * NB;
+    const int32_t rs = (kb + 1) * NB;  // trailing start
+    const int32_t r0 = rs + ti * ST, c0 = rs + tj * ST, k0 = kb * NB;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+    for (int idx = tid; idx < ST * NB; idx += 256) {
         const int i = idx / NB, m = idx % NB;
-        at[m][i] = (r0 + i < n) ? L[(int64_t)(r0 + i) * n + k0 + m] : 0.0;
-        bt[m][i] = (cc0 + i < n) ? L[(int64_t)(cc0 + i) * n + k0 + m] : 0.0;
+        at[m * SP + i] = (r0 + i < n) ? L[(int64_t)(r0 + i) * n + k0 + m] : 0.0;
+        bt[m * SP + i] = (c0 + i < n) ? L[(int64_t)(c0 + i) * n + k0 + m] : 0.0;
     }
     __syncthreads();
     const int tx = tid % 16, ty = tid / 16;
-    double acc[4][4] = {};
-#pragma unroll 4
+    double acc[8][8];
+#pragma unroll
+    for (int p = 0; p < 8; p++)
+#pragma unroll
+        for (int q = 0; q < 8; q++) acc[p][q] = 0.0;
+#pragma unroll 2
     for (int m = 0; m < NB; m++) {
-        const double2 a01 = *reinterpret_cast<const double2*>(&at[m][ty * 4]);
-        const double2 a23 = *reinterpret_cast<const double2*>(&at[m][ty * 4 + 2]);
-        const double2 b01 = *reinterpret_cast<const double2*>(&bt[m][tx * 4]);
-        const double2 b23 = *reinterpret_cast<const double2*>(&bt[m][tx * 4 + 2]);
-        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-        for (int p = 0; p < 4; p++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) acc[p][q] += av[p] * bv[q];
-    }
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-        const int32_t i = r0 + ty * 4 + p;
-        if (i >= n) continue;
+        double av[8], bv[8];
+        const double2* ap = reinterpret_cast<const double2*>(at + m * SP + ty * 8);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const int32_t c = cc0 + tx * 4 + q;
-            if (c < n && c <= i) L[(int64_t)i * n + c] -= acc[p][q];
+            // columns 2*tx + 32*q + {0,1}: a warp's 16 lanes read 256 contiguous bytes
+            const double2 a2 = ap[q];
+            const double2 b2 = *reinterpret_cast<const double2*>(bt + m * SP + 32 * q + 2 * tx);
+            av[2 * q] = a2.x;
+            av[2 * q + 1] = a2.y;
+            bv[2 * q] = b2.x;
+            bv[2 * q + 1] = b2.y;
+        }
+#pragma unroll
+        for (int p = 0; p < 8; p++)
+#pragma unroll
+            for (int q = 0; q < 8; q++) acc[p][q] = fma(av[p], bv[q], acc[p][q]);
+    }
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        const int32_t i = r0 + ty * 8 + p;
+        if (i >= n) continue;
+        double* row = L + (int64_t)i * n;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int32_t c = c0 + 32 * (q >> 1) + 2 * tx + (q & 1);
+            if (c < n && c <= i) row[c] -= acc[p][q];
         }
     }
 }
 
 // ---- triangular solves: B[nrhs][n] ------------------------------------------
 
-// Forward block step kb: y_kb = inv(L_kk) b_kb (every CTA recomputes it), CTA 0
-// stores it into Y; rows of later blocks assigned to this CTA get
-// b_j -= L_j,kb y_kb.
+// Triangular-solve block steps. Dynamic shared memory: the 64x64 diagonal
+// inverse, one 64x64 tile of L and the block of right-hand sides, all staged
+// with coalesced loads.
+constexpr int TP = NB + 1;
+
+// Forward step kb: y = inv(L_kk) b_kk (every CTA recomputes it from shared
+// memory), CTA 0 stores y into Y; CTA j updates the 64 rows after block kb it
+// owns: b_row -= L[row][kb block] y.
 __global__ void __launch_bounds__(256)
 trsv_fwd_kernel(const double* __restrict__ L, const double* __restrict__ Linv, int32_t n,
                 int32_t kb, double* __restrict__ B, double* __restrict__ Y, int32_t nrhs) {
     extern __shared__ double sm[];
-    double* y = sm;  // [nrhs][NB]
+    double* li = sm;              // [NB][TP]
+    double* lt = li + NB * TP;    // [NB][TP]
+    double* bb = lt + NB * TP;    // [nrhs][NB]
+    double* y = bb + nrhs * NB;   // [nrhs][NB]
     const int32_t r0 = kb * NB;
     const int32_t s = min(NB, n - r0);
-    const double* Li = Linv + (int64_t)kb * NB * NB;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < nrhs * NB; idx += blockDim.x) {
+    const double* Li = Linv + (int64_t)kb * NB * NB;
+    for (int idx = tid; idx < NB * NB; idx += 256) li[(idx / NB) * TP + idx % NB] = Li[idx];
+    for (int idx = tid; idx < nrhs * NB; idx += 256) {
+        const int q = idx / NB, m = idx % NB;
+        bb[idx] = (m < s) ? B[(int64_t)q * n + r0 + m] : 0.0;
+    }
+    const int32_t row0 = r0 + NB + blockIdx.x * NB;
+    for (int idx = tid; idx < NB * NB; idx += 256) {
+        const int rr = idx / NB, m = idx % NB;
+        lt[rr * TP + m] = (row0 + rr < n && m < s) ? L[(int64_t)(row0 + rr) * n + r0 + m] : 0.0;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nrhs * NB; idx += 256) {
         const int q = idx / NB, i = idx % NB;
         double acc = 0.0;
-        if (i < s)
-            for (int m = 0; m <= i; m++) acc += Li[i * NB + m] * B[(int64_t)q * n + r0 + m];
-        y[q * NB + i] = acc;
+        for (int m = 0; m <= i; m++) acc += li[i * TP + m] * bb[q * NB + m];
+        y[idx] = acc;
     }
     __syncthreads();
     if (blockIdx.x == 0)
-        for (int idx = tid; idx < nrhs * s; idx += blockDim.x) {
-            const int q = idx / s, i = idx % s;
-            Y[(int64_t)q * n + r0 + i] = y[q * NB + i];
+        for (int idx = tid; idx < nrhs * NB; idx += 256) {
+            const int q = idx / NB, i = idx % NB;
+            if (i < s) Y[(int64_t)q * n + r0 + i] = y[idx];
         }
-    // rows after this block: 64 rows per CTA
-    const int32_t row0 = r0 + NB + blockIdx.x * NB;
-    for (int idx = tid; idx < NB * nrhs; idx += blockDim.x) {
-        const int rr = idx % NB, q = idx / NB;
-        const int32_t j = row0 + rr;
-        if (j >= n) continue;
-        const double* Lj = L + (int64_t)j * n + r0;
+    if (row0 >= n) return;
+    for (int idx = tid; idx < nrhs * NB; idx += 256) {
+        const int q = idx / NB, rr = idx % NB;
+        if (row0 + rr >= n) continue;
         double acc = 0.0;
-        for (int m = 0; m < s; m++) acc += Lj[m] * y[q * NB + m];
-        B[(int64_t)q * n + j] -= acc;
+#pragma unroll 8
+        for (int m = 0; m < NB; m++) acc += lt[rr * TP + m] * y[q * NB + m];
+        B[(int64_t)q * n + row0 + rr] -= acc;
     }
 }
 
-// Backward block step kb: x_kb = inv(L_kk)^T y_kb, stored into X; columns of
-// earlier blocks assigned to this CTA get y_c -= sum_r L[kb*64+r][c] x_r.
+// Backward step kb: x = inv(L_kk)^T y_kk, CTA 0 stores x into X; CTA j updates
+// the 64 columns it owns before block kb: y_c -= sum_r L[kb*64 + r][c] x_r.
 __global__ void __launch_bounds__(256)
 trsv_bwd_kernel(const double* __restrict__ L, const double* __restrict__ Linv, int32_t n,
                 int32_t kb, double* __restrict__ Yv, double* __restrict__ X, int32_t nrhs) {
     extern __shared__ double sm[];
-    double* x = sm;  // [nrhs][NB]
+    double* li = sm;
+    double* lt = li + NB * TP;
+    double* yb = lt + NB * TP;
+    double* x = yb + nrhs * NB;
     const int32_t r0 = kb * NB;
     const int32_t s = min(NB, n - r0);
-    const double* Li = Linv + (int64_t)kb * NB * NB;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < nrhs * NB; idx += blockDim.x) {
+    const double* Li = Linv + (int64_t)kb * NB * NB;
+    for (int idx = tid; idx < NB * NB; idx += 256) li[(idx / NB) * TP + idx % NB] = Li[idx];
+    for (int idx = tid; idx < nrhs * NB; idx += 256) {
+        const int q = idx / NB, m = idx % NB;
+        yb[idx] = (m < s) ? Yv[(int64_t)q * n + r0 + m] : 0.0;
+    }
+    const int32_t col0 = blockIdx.x * NB;
+    const bool upd = col0 < r0;
+    if (upd)
+        for (int idx = tid; idx < NB * NB; idx += 256) {
+            const int r = idx / NB, cc = idx % NB;
+            lt[r * TP + cc] = (r < s) ? L[(int64_t)(r0 + r) * n + col0 + cc] : 0.0;
+        }
+    __syncthreads();
+    for (int idx = tid; idx < nrhs * NB; idx += 256) {
         const int q = idx / NB, i = idx % NB;
         double acc = 0.0;
-        if (i < s)
-            for (int m = i; m < s; m++) acc += Li[m * NB + i] * Yv[(int64_t)q * n + r0 + m];
-        x[q * NB + i] = acc;
+        for (int m = i; m < NB; m++) acc += li[m * TP + i] * yb[q * NB + m];
+        x[idx] = acc;
     }
     __syncthreads();
     if (blockIdx.x == 0)
-        for (int idx = tid; idx < nrhs * s; idx += blockDim.x) {
-            const int q = idx / s, i = idx % s;
-            X[(int64_t)q * n + r0 + i] = x[q * NB + i];
+        for (int idx = tid; idx < nrhs * NB; idx += 256) {
+            const int q = idx / NB, i = idx % NB;
+            if (i < s) X[(int64_t)q * n + r0 + i] = x[idx];
         }
-    const int32_t col0 = blockIdx.x * NB;
-    if (col0 >= r0) return;
-    for (int idx = tid; idx < NB * nrhs; idx += blockDim.x) {
-        const int cc = idx % NB, q = idx / NB;
-        const int32_t c = col0 + cc;
-        if (c >= r0) continue;
+    if (!upd) return;
+    for (int idx = tid; idx < nrhs * NB; idx += 256) {
+        const int q = idx / NB, cc = idx % NB;
         double acc = 0.0;
-        for (int r = 0; r < s; r++) acc += L[(int64_t)(r0 + r) * n + c] * x[q * NB + r];
-        Yv[(int64_t)q * n + c] -= acc;
+#pragma unroll 8
+        for (int r = 0; r < NB; r++) acc += lt[r * TP + cc] * x[q * NB + r];
+        Yv[(int64_t)q * n + col0 + cc] -= acc;
     }
 }
 
@@ -424,7 +469,7 @@ int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, doub
     int32_t* st = ctx->status.as<int32_t>();
     TPE_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(int32_t), ctx->stream));
     const size_t sm1 = sizeof(double) * 2 * NB * (NB + 1);
-    const size_t sm2 = sizeof(double) * 2 * NB * (NB + 2);
+    const size_t sm2 = sizeof(double) * 2 * NB * SP;
     TPE_CUDA_TRY(cudaFuncSetAttribute(potrf_diag_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
     TPE_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel,
@@ -437,7 +482,8 @@ int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, doub
         const int32_t rest = nb - kb - 1;
         if (rest > 0) {
             trsm_panel_kernel<<<rest, 256, sm1, ctx->stream>>>(d_L, d_Linv, n, kb);
-            const int64_t tiles = (int64_t)rest * (rest + 1) / 2;
+            const int64_t nt2 = ((int64_t)rest * NB + ST - 1) / ST;
+            const int64_t tiles = nt2 * (nt2 + 1) / 2;
             syrk_update_kernel<<<(unsigned)tiles, 256, sm2, ctx->stream>>>(d_L, n, kb);
         }
     }
@@ -455,11 +501,15 @@ int32_t chol_solve_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, i
     const int32_t nb = (n + NB - 1) / NB;
     TPE_TRY(ensure(ctx, ctx->solve_scratch, sizeof(double) * (size_t)n * nrhs));
     double* Y = ctx->solve_scratch.as<double>();
-    const size_t smem = sizeof(double) * (size_t)nrhs * NB;
-    if (smem > 48 * 1024) {
-        set_error(ctx, TPE_ERR_TOO_LARGE, "chol_solve: too many right-hand sides per call");
+    const size_t smem = sizeof(double) * (2 * (size_t)NB * TP + 2 * (size_t)nrhs * NB);
+    if (nrhs > 64) {
+        set_error(ctx, TPE_ERR_TOO_LARGE, "chol_solve: at most 64 right-hand sides per call");
         return TPE_ERR_TOO_LARGE;
     }
+    TPE_CUDA_TRY(cudaFuncSetAttribute(trsv_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(double) * (2 * NB * TP + 2 * 64 * NB))));
+    TPE_CUDA_TRY(cudaFuncSetAttribute(trsv_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(double) * (2 * NB * TP + 2 * 64 * NB))));
     KernelScope ks(ctx, TPE_KGROUP_TRSV, 2 * (int64_t)nb);
     for (int32_t kb = 0; kb < nb; kb++) {
         const int32_t rows_after = n - (kb + 1) * NB;

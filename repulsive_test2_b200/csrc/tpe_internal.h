@@ -52,6 +52,8 @@ struct SaddleOp {
     double* Linv = nullptr;  // nb x 64 x 64 inverses of the diagonal blocks of L
     double* C = nullptr;     // k x 3V dense constraint Jacobian
     double* Y = nullptr;     // k x 3V: Abar_rho^{-1} C^T (row s = column s of C^T)
+    double* W = nullptr;     // 3V: Abar_rho^{-1} b for the b given at factor time (row k of Y)
+    const double* w_src = nullptr;  // that b (device), or null
     // host: small Schur complement and its factors
     std::vector<double> Scc;   // k x k, then its Cholesky factor (lower)
     std::vector<double> Scu;   // k x 3 = C U / rho
