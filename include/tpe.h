@@ -233,6 +233,23 @@ int32_t tpe_penalty_gradient(tpe_ctx* ctx, const double* xyz, const tpe_penaltie
 int32_t tpe_energy_batch(tpe_ctx* ctx, const double* xyz, int32_t ncurves, const tpe_params* p,
                          int32_t precision, double* energies);
 
+/* ---- allocation-free energy (no counterpart in the reference) --------------- */
+/* calculateEnergy for callers that cannot call cudaMalloc: a loop being
+ * captured into a CUDA graph, an application whose device memory comes only
+ * from its own allocator, a real-time loop that must not hit the allocator.
+ * d_xyz (V x 3 FP64) and d_edges (E x 2 int32) are device pointers on the
+ * current device, d_energy receives one double there; `stream` is a
+ * cudaStream_t (NULL = the legacy default stream). No context is created and
+ * nothing is allocated: the scratch is a static device array of about 1 MiB
+ * that every GPU loading the library holds until exit, so E is limited to
+ * 16384 (larger E returns TPE_ERR_TOO_LARGE). The first call on a device looks
+ * up the scratch's device address (cudaGetSymbolAddress), so make that first
+ * call before any stream capture. All calls share the one scratch array: calls
+ * that overlap on the GPU (different streams, or different host threads)
+ * race; serialise them. */
+int32_t tpe_energy_noalloc(const double* d_xyz, const int32_t* d_edges, int32_t V, int32_t E,
+                           const tpe_params* p, double* d_energy, void* stream);
+
 /* ---- device-resident step and instrumentation (extensions) ------------------ */
 /* sobolevStepSet with the vertices already in device memory (d_xyz, d_xyz_out
  * are V x 3 device pointers on this context's device); for callers that keep

@@ -156,6 +156,8 @@ SIGNATURES = {
                                             C.POINTER(tpe_step_opts), C.c_void_p,
                                             C.POINTER(tpe_step_stats), dp]),
     "tpe_stream": (C.c_void_p, [vp]),
+    "tpe_energy_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(tpe_params),
+                                       C.c_void_p, C.c_void_p]),
     "tpe_profile": (C.c_int32, [vp, C.c_int32]),
     "tpe_profile_read": (C.c_int32, [vp, dp, C.POINTER(C.c_int64)]),
 }

@@ -374,6 +374,33 @@ int32_t energy_fp64(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, do
     return TPE_OK;
 }
 
+// Energy of one curve with caller-provided scratch (no context, no allocation):
+// edge records ea/eb (E each) and partial[max_parts]. Returns TPE_ERR_TOO_LARGE if
+// the partials do not fit. The J range is split into at most 16 chunks.
+int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2* d_edges,
+                            int32_t V, int32_t E, double alpha, double beta, double eps,
+                            double4* ea, double4* eb, double* partial, int32_t max_parts,
+                            double* d_energy) {
+    const int32_t xb = (E + kThreads - 1) / kThreads;
+    int32_t ny = (E + kTile - 1) / kTile;
+    ny = ny < 16 ? ny : 16;
+    const int32_t jchunk = ((E + ny - 1) / ny + kTile - 1) / kTile * kTile;
+    const int32_t nyy = (E + jchunk - 1) / jchunk;
+    const int32_t nparts = xb * nyy;
+    if (nparts > max_parts) return TPE_ERR_TOO_LARGE;
+    edge_prep_kernel<<<(E + 255) / 256, 256, 0, stream>>>(d_pos, d_edges, E, V, 1, eps, alpha, ea,
+                                                          eb);
+    dim3 grid(xb, nyy, 1);
+    if (exp_mode(alpha, beta) == 1)
+        energy_kernel<1><<<grid, kThreads, 0, stream>>>(ea, eb, d_edges, E, jchunk, alpha, beta,
+                                                        eps, partial);
+    else
+        energy_kernel<0><<<grid, kThreads, 0, stream>>>(ea, eb, d_edges, E, jchunk, alpha, beta,
+                                                        eps, partial);
+    reduce_partials<<<1, 256, 0, stream>>>(partial, nparts, 0.125, d_energy);
+    return cudaGetLastError() == cudaSuccess ? TPE_OK : TPE_ERR_CUDA;
+}
+
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
                          double* d_grad) {
     const int32_t E = ctx->E, V = ctx->V;

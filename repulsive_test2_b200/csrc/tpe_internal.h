@@ -133,6 +133,11 @@ int32_t edge_prep(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps
 // d_energy[ncurves] (device).
 int32_t energy_fp64(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, double eps,
                     double* d_energy);
+// Energy of one curve with caller-provided scratch and stream (no context).
+int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2* d_edges,
+                            int32_t V, int32_t E, double alpha, double beta, double eps,
+                            double4* ea, double4* eb, double* partial, int32_t max_parts,
+                            double* d_energy);
 // Energy (optional) and gradient (interleaved V x 3) of one curve.
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
                          double* d_grad);
