@@ -428,13 +428,18 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
 // Assemble A and C at device positions d_pos (set already uploaded) and factor.
 int32_t op_build(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k, double alpha,
                  double beta, double eps, bool* singular, double* timings,
-                 const double* b_flat = nullptr) {
+                 const double* b_flat = nullptr, int32_t precision = TPE_PRECISION_FP64) {
     const int32_t V = ctx->V;
     {
         Timer t(ctx, timings, TPE_PHASE_ASSEMBLEA);
         TPE_TRY(ensure(ctx, ctx->mat_A, sizeof(double) * (size_t)V * V));
-        TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
-        TPE_TRY(assemble_fp64(ctx, alpha, beta, eps, ctx->mat_A.as<double>(), nullptr, nullptr));
+        if (precision == TPE_PRECISION_MIXED) {
+            TPE_TRY(edge_prep_mixed(ctx, d_pos, 1, eps, alpha));
+            TPE_TRY(assemble_mixed(ctx, alpha, beta, eps, ctx->mat_A.as<double>()));
+        } else {
+            TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
+            TPE_TRY(assemble_fp64(ctx, alpha, beta, eps, ctx->mat_A.as<double>(), nullptr, nullptr));
+        }
     }
     TPE_TRY(ensure(ctx, ctx->con_C, sizeof(double) * (size_t)(k > 0 ? k : 1) * 3 * V));
     std::vector<double> phi, ns;
@@ -521,11 +526,16 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
 // ---- energies -------------------------------------------------------------------
 
 int32_t energy_of(tpe_ctx* ctx, const double* d_pos, double alpha, double beta, double eps,
-                  double* out) {
-    TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
+                  double* out, int32_t precision = TPE_PRECISION_FP64) {
     TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * 600));
     double* de = ctx->scalars.as<double>() + 520;
-    TPE_TRY(energy_fp64(ctx, 1, alpha, beta, eps, de));
+    if (precision == TPE_PRECISION_MIXED) {
+        TPE_TRY(edge_prep_mixed(ctx, d_pos, 1, eps, alpha));
+        TPE_TRY(energy_mixed(ctx, 1, alpha, beta, eps, de));
+    } else {
+        TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
+        TPE_TRY(energy_fp64(ctx, 1, alpha, beta, eps, de));
+    }
     return download(ctx, out, de, sizeof(double));
 }
 
@@ -534,7 +544,7 @@ int32_t objective(tpe_ctx* ctx, const double* d_pos, const tpe_step_opts* o, boo
     double e = 0.0;
     {
         Timer t(ctx, timings, TPE_PHASE_ENERGY);
-        TPE_TRY(energy_of(ctx, d_pos, o->alpha, o->beta, o->epsilon, &e));
+        TPE_TRY(energy_of(ctx, d_pos, o->alpha, o->beta, o->epsilon, &e, o->precision));
     }
     if (pen) {
         double pe = 0.0;
@@ -628,7 +638,7 @@ int32_t project_dev(tpe_ctx* ctx, const double* d_start, const SetInfo& S, const
         if (!frozen) {
             bool singular = false;
             TPE_TRY(op_build(ctx, d_cur, S.nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular,
-                             timings));
+                             timings, nullptr, o->precision));
             if (singular) {
                 *iters = it;
                 break;
@@ -820,7 +830,13 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
     }
     tpe_ctx* ctx = new tpe_ctx();
     ctx->device = device;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    // The main stream carries the factorization's critical path: give it the
+    // highest priority so its small kernels are scheduled ahead of the
+    // look-ahead stream's large trailing updates.
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
         delete ctx;
         if (status) *status = TPE_ERR_CUDA;
         return nullptr;
@@ -837,7 +853,7 @@ void tpe_destroy(tpe_ctx* ctx) {
     DevBuf* bufs[] = {&ctx->d_edges, &ctx->d_inc_off, &ctx->d_inc, &ctx->pos, &ctx->pos2,
                       &ctx->pos3, &ctx->edge_a, &ctx->edge_b, &ctx->grad, &ctx->edge_acc,
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
-                      &ctx->flat3, &ctx->dir, &ctx->pairM, &ctx->mat_A, &ctx->mat_L,
+                      &ctx->flat3, &ctx->dir, &ctx->pairM, &ctx->edge_m, &ctx->mat_A, &ctx->mat_L,
                       &ctx->mat_Linv, &ctx->mat_B, &ctx->mat_B0, &ctx->con_C, &ctx->con_Y,
                       &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->rhs,
                       &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status};
@@ -848,6 +864,8 @@ void tpe_destroy(tpe_ctx* ctx) {
         cudaEventDestroy(p.b);
     }
     for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->fac_events) cudaEventDestroy(e);
+    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1162,6 +1180,9 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
         Timer t(ctx, timings, TPE_PHASE_DE);
         if (o->mode == TPE_DE_FINITE_DIFF) {
             TPE_TRY(gradient_fd_dev(ctx, P, o->alpha, o->beta, o->epsilon, o->h, dE));
+        } else if (o->precision == TPE_PRECISION_MIXED) {
+            TPE_TRY(edge_prep_mixed(ctx, P, 1, o->epsilon, o->alpha));
+            TPE_TRY(energy_grad_mixed(ctx, o->alpha, o->beta, o->epsilon, nullptr, dE));
         } else {
             TPE_TRY(edge_prep(ctx, P, 1, o->epsilon, o->alpha));
             TPE_TRY(energy_grad_fp64(ctx, o->alpha, o->beta, o->epsilon, nullptr, dE));
@@ -1172,7 +1193,7 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
     TPE_TRY(interleaved_to_block(ctx, dE, ctx->flat2.as<double>(), V));
     bool singular = false;
     TPE_TRY(op_build(ctx, P, nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular, timings,
-                     ctx->flat2.as<double>()));
+                     ctx->flat2.as<double>(), o->precision));
     TPE_TRY(ensure(ctx, ctx->sol, sizeof(double) * m));
     double* out = ctx->sol.as<double>();
     if (singular) {
@@ -1328,14 +1349,18 @@ int32_t tpe_penalty_gradient(tpe_ctx* ctx, const double* xyz, const tpe_penaltie
 int32_t tpe_energy_batch(tpe_ctx* ctx, const double* xyz, int32_t ncurves, const tpe_params* p,
                          int32_t precision, double* energies) {
     TPE_TRY(check_topology(ctx));
-    (void)precision;
     if (!xyz || !p || !energies || ncurves <= 0) return TPE_ERR_BAD_ARG;
     const size_t m = 3 * (size_t)ctx->V;
     TPE_TRY(upload(ctx, ctx->pos3, xyz, sizeof(double) * m * ncurves));
-    TPE_TRY(edge_prep(ctx, ctx->pos3.as<double>(), ncurves, p->epsilon, p->alpha));
     TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * (600 + (size_t)ncurves)));
     double* de = ctx->scalars.as<double>() + 600;
-    TPE_TRY(energy_fp64(ctx, ncurves, p->alpha, p->beta, p->epsilon, de));
+    if (precision == TPE_PRECISION_MIXED) {
+        TPE_TRY(edge_prep_mixed(ctx, ctx->pos3.as<double>(), ncurves, p->epsilon, p->alpha));
+        TPE_TRY(energy_mixed(ctx, ncurves, p->alpha, p->beta, p->epsilon, de));
+    } else {
+        TPE_TRY(edge_prep(ctx, ctx->pos3.as<double>(), ncurves, p->epsilon, p->alpha));
+        TPE_TRY(energy_fp64(ctx, ncurves, p->alpha, p->beta, p->epsilon, de));
+    }
     return download(ctx, energies, de, sizeof(double) * ncurves);
 }
 

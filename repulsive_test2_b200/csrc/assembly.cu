@@ -236,6 +236,18 @@ __global__ void gather_A_kernel(const double2* __restrict__ M, int32_t E,
 
 }  // namespace
 
+int32_t gather_A_launch(tpe_ctx* ctx, double* d_A, double* d_B, double* d_B0) {
+    const int32_t V = ctx->V, E = ctx->E;
+    const int32_t nt = (V + 31) / 32;
+    const int32_t tiles = nt * (nt + 1) / 2;
+    KernelScope ks(ctx, TPE_KGROUP_GATHER_A, 1);
+    gather_A_kernel<<<tiles, dim3(32, 32), 0, ctx->stream>>>(
+        ctx->pairM.as<double2>(), E, ctx->d_inc_off.as<int32_t>(), ctx->d_inc.as<int32_t>(), V,
+        tiles, d_A, d_B, d_B0);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
 int32_t assemble_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_A,
                       double* d_B, double* d_B0) {
     const int32_t E = ctx->E, V = ctx->V;
@@ -261,13 +273,7 @@ int32_t assemble_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, doubl
             ctx->edge_a.as<double4>(), E, ntp, ctx->tmp.as<double2>(), ctx->pairM.as<double2>());
         TPE_CUDA_TRY(cudaGetLastError());
     }
-    const int32_t nt = (V + 31) / 32;
-    KernelScope ks(ctx, TPE_KGROUP_GATHER_A, 1);
-    const int32_t tiles = nt * (nt + 1) / 2;
-    gather_A_kernel<<<tiles, dim3(32, 32), 0, ctx->stream>>>(
-        ctx->pairM.as<double2>(), E, ctx->d_inc_off.as<int32_t>(), ctx->d_inc.as<int32_t>(), V,
-        tiles, d_A, d_B, d_B0);
-    TPE_CUDA_TRY(cudaGetLastError());
+    return gather_A_launch(ctx, d_A, d_B, d_B0);
     return TPE_OK;
 }
 

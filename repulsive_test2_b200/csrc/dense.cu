@@ -9,9 +9,12 @@
 // and a tiled kernel applies the symmetric rank-64 update to the trailing
 // lower triangle. Triangular solves run block row by block row with the same
 // diagonal-block inverses.
+#include <cooperative_groups.h>
 #include <math.h>
 
 #include "tpe_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace tpe {
 namespace {
@@ -20,68 +23,123 @@ constexpr int NB = kNB;  // 64
 
 // ---- Cholesky --------------------------------------------------------------
 
-// One CTA (256 threads): factor the diagonal block kb (size s <= 64) of the
-// lower triangle in place and write its inverse into Linv[kb].
+// One CTA (256 threads): factor the 64x64 diagonal block kb (size s <= 64,
+// padded with the identity) in FP64 and write L_kk and inv(L_kk). The block is
+// processed in four 16-column panels: warp 0 factors a panel in registers
+// (lane l owns panel rows c0+l and c0+l+32, column entries broadcast with
+// shuffles), then all warps apply the rank-16 update to the rest of the block.
+// The inverse is built from 16x16 diagonal inverses and three block-diagonal
+// stages X_ij = -inv(L_ii) sum_{m=j}^{i-1} L_im X_mj. About 15 barriers in all.
+template <typename T>
 __global__ void __launch_bounds__(256)
-potrf_diag_kernel(double* __restrict__ L, double* __restrict__ Linv, int32_t n, int32_t kb,
-                  double tol, int32_t* __restrict__ status) {
+potrf_diag_kernel(T* __restrict__ L, T* __restrict__ Linv, int32_t n, int32_t kb, double tol,
+                  int32_t* __restrict__ status) {
     extern __shared__ double dsm[];
     double(*a)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);
     double(*inv)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + NB * (NB + 1));
+    double(*tmp)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + 2 * NB * (NB + 1));
     __shared__ int bad;
     const int32_t r0 = kb * NB;
     const int32_t s = min(NB, n - r0);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) bad = 0;
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+    for (int idx = tid; idx < NB * NB; idx += 256) {
         const int i = idx / NB, j = idx % NB;
         double v;
         if (i < s && j < s)
-            v = (j <= i) ? L[(int64_t)(r0 + i) * n + r0 + j] : 0.0;
+            v = (j <= i) ? (double)L[(int64_t)(r0 + i) * n + r0 + j] : 0.0;
         else
             v = (i == j) ? 1.0 : 0.0;
         a[i][j] = v;
+        inv[i][j] = 0.0;
     }
     __syncthreads();
-    for (int j = 0; j < NB; j++) {
-        if (tid == 0) {
-            const double d = a[j][j];
-            if (!(d > tol)) {
-                bad = 1;
-                a[j][j] = 1.0;
-            } else {
-                a[j][j] = sqrt(d);
+    for (int p = 0; p < 4; p++) {
+        const int c0 = 16 * p;
+        if (warp == 0) {
+            const int ra = c0 + lane, rb = c0 + lane + 32;
+            const bool va = ra < NB, vb = rb < NB;
+            double x[16], y[16];
+#pragma unroll
+            for (int c = 0; c < 16; c++) {
+                x[c] = va ? a[ra][c0 + c] : 0.0;
+                y[c] = vb ? a[rb][c0 + c] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                double d = __shfl_sync(0xffffffffu, x[j], j);
+                if (!(d > tol)) {
+                    if (lane == 0) bad = 1;
+                    d = 1.0;
+                }
+                const double sq = sqrt(d);
+                const double iv = 1.0 / sq;
+                if (lane > j) x[j] *= iv;
+                if (lane == j) x[j] = sq;
+                y[j] *= iv;
+#pragma unroll
+                for (int c = j + 1; c < 16; c++) {
+                    const double lcj = __shfl_sync(0xffffffffu, x[j], c);
+                    if (lane >= c) x[c] -= x[j] * lcj;
+                    y[c] -= y[j] * lcj;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 16; c++) {
+                if (va && ra >= c0 + c) a[ra][c0 + c] = x[c];
+                if (vb) a[rb][c0 + c] = y[c];
             }
         }
         __syncthreads();
-        const double djj = a[j][j];
-        for (int i = j + 1 + tid; i < NB; i += blockDim.x) a[i][j] /= djj;
-        __syncthreads();
-        // trailing update of the lower triangle: a[i][c] -= a[i][j] * a[c][j], j < c <= i
-        const int m = NB - j - 1;
-        for (int idx = tid; idx < m * m; idx += blockDim.x) {
-            const int i = j + 1 + idx / m, c = j + 1 + idx % m;
-            if (c <= i) a[i][c] -= a[i][j] * a[c][j];
+        const int c1 = c0 + 16, m = NB - c1;
+        if (m > 0) {
+            for (int idx = tid; idx < m * m; idx += 256) {
+                const int i = c1 + idx / m, c = c1 + idx % m;
+                if (c > i) continue;
+                double acc = a[i][c];
+#pragma unroll
+                for (int q = 0; q < 16; q++) acc -= a[i][c0 + q] * a[c][c0 + q];
+                a[i][c] = acc;
+            }
         }
         __syncthreads();
     }
-    // inverse of the lower-triangular factor, one column per thread
-    if (tid < NB) {
-        const int c = tid;
-        for (int i = 0; i < NB; i++) inv[i][c] = 0.0;
-        inv[c][c] = 1.0 / a[c][c];
-        for (int i = c + 1; i < NB; i++) {
-            double acc = 0.0;
-            for (int m2 = c; m2 < i; m2++) acc += a[i][m2] * inv[m2][c];
-            inv[i][c] = -acc / a[i][i];
+    // 16x16 diagonal inverses: warp w < 4 inverts block w, lane c < 16 owns column c
+    if (warp < 4 && lane < 16) {
+        const int o = 16 * warp, c = lane;
+        for (int i = 0; i < 16; i++) {
+            double acc = (i == c) ? 1.0 : 0.0;
+            for (int mm = c; mm < i; mm++) acc -= a[o + i][o + mm] * inv[o + mm][o + c];
+            inv[o + i][o + c] = (i >= c) ? acc / a[o + i][o + i] : 0.0;
         }
     }
     __syncthreads();
-    double* Li = Linv + (int64_t)kb * NB * NB;
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+    for (int dgl = 1; dgl < 4; dgl++) {
+        // tmp_ij = sum_{m=j}^{i-1} L_im X_mj for the blocks (i, j = i - dgl)
+        const int nblk = 4 - dgl;
+        for (int idx = tid; idx < nblk * 256; idx += 256) {
+            const int bi = idx / 256, e = idx % 256, r = e / 16, c = e % 16;
+            const int i = bi + dgl, j = bi;
+            double acc = 0.0;
+            for (int mb = j; mb < i; mb++)
+                for (int q = 0; q < 16; q++) acc += a[16 * i + r][16 * mb + q] * inv[16 * mb + q][16 * j + c];
+            tmp[16 * i + r][16 * j + c] = acc;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < nblk * 256; idx += 256) {
+            const int bi = idx / 256, e = idx % 256, r = e / 16, c = e % 16;
+            const int i = bi + dgl, j = bi;
+            double acc = 0.0;
+            for (int q = 0; q < 16; q++) acc += inv[16 * i + r][16 * i + q] * tmp[16 * i + q][16 * j + c];
+            inv[16 * i + r][16 * j + c] = -acc;
+        }
+        __syncthreads();
+    }
+    T* Li = Linv + (int64_t)kb * NB * NB;
+    for (int idx = tid; idx < NB * NB; idx += 256) {
         const int i = idx / NB, j = idx % NB;
-        Li[idx] = inv[i][j];
-        if (i < s && j < s && j <= i) L[(int64_t)(r0 + i) * n + r0 + j] = a[i][j];
+        Li[idx] = (T)inv[i][j];
+        if (i < s && j < s && j <= i) L[(int64_t)(r0 + i) * n + r0 + j] = (T)a[i][j];
     }
     if (tid == 0 && bad) atomicOr(status, 1);
 }
@@ -126,171 +184,202 @@ trsm_panel_kernel(double* __restrict__ L, const double* __restrict__ Linv, int32
     }
 }
 
-// Trailing update A_ij -= L_ik L_jk^T over the lower triangle of the trailing
-// matrix, in 128 x 128 tiles (rank-64 update, K = the panel). 256 threads, each
-// an 8 x 8 register tile; the two 128 x 64 panels are staged transposed in
-// shared memory; a thread owns rows 8ty..8ty+7 and columns 2tx + 32q + {0,1}.
-constexpr int ST = 128;
-constexpr int SP = ST + 2;
+// Lower-triangle update L[r][c] -= sum_{m<kl} L[r][k0+m] L[c][k0+m] for
+// r in [r_s, n), c in [c_s, c_e), c <= r, on the FP64 tensor cores
+// (mma.sync m8n8k4 f64). 128x128 output tiles (tiles entirely above the
+// diagonal exit at once), 8 warps as 2 (rows) x 4 (cols), each warp 64x32 =
+// 8x4 MMA tiles. K runs in chunks of 32 staged by 16-byte cp.async into two
+// shared-memory buffers; rows are padded to 36 doubles (72 words = 8 banks
+// mod 32) so a fragment load (8 rows x 4 k) takes the minimum two wavefronts.
+constexpr int GT = 128;
+constexpr int GK = 32;
+constexpr int GP = GK + 4;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 __global__ void __launch_bounds__(256)
-syrk_update_kernel(double* __restrict__ L, int32_t n, int32_t kb) {
+gemm_lower_update_kernel(double* __restrict__ L, int32_t n, int32_t r_s, int32_t c_s, int32_t c_e,
+                         int32_t k0, int32_t kl) {
     extern __shared__ double dsm[];
-    double* at = dsm;            // at[m * SP + r] = L[r0 + r][k0 + m]
-    double* bt = dsm + NB * SP;  // bt[m * SP + c] = L[c0 + c][k0 + m]
-    const int64_t t = blockIdx.x;
-    int32_t ti = (int32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((int64_t)ti * (ti + 1) / 2 > t) ti--;
-    while ((int64_t)(ti + 1) * (ti + 2) / 2 <= t) ti++;
-    const int32_t tj = (int32_t)(t - (int64_t)ti * (ti + 1) / 2);
-    const int32_t rs = (kb + 1) * NB;  // trailing start
-    const int32_t r0 = rs + ti * ST, c0 = rs + tj * ST, k0 = kb * NB;
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < ST * NB; idx += 256) {
-        const int i = idx / NB, m = idx % NB;
-        at[m * SP + i] = (r0 + i < n) ? L[(int64_t)(r0 + i) * n + k0 + m] : 0.0;
-        bt[m * SP + i] = (c0 + i < n) ? L[(int64_t)(c0 + i) * n + k0 + m] : 0.0;
-    }
-    __syncthreads();
-    const int tx = tid % 16, ty = tid / 16;
-    double acc[8][8];
-#pragma unroll
-    for (int p = 0; p < 8; p++)
-#pragma unroll
-        for (int q = 0; q < 8; q++) acc[p][q] = 0.0;
-#pragma unroll 2
-    for (int m = 0; m < NB; m++) {
-        double av[8], bv[8];
-        const double2* ap = reinterpret_cast<const double2*>(at + m * SP + ty * 8);
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            // columns 2*tx + 32*q + {0,1}: a warp's 16 lanes read 256 contiguous bytes
-            const double2 a2 = ap[q];
-            const double2 b2 = *reinterpret_cast<const double2*>(bt + m * SP + 32 * q + 2 * tx);
-            av[2 * q] = a2.x;
-            av[2 * q + 1] = a2.y;
-            bv[2 * q] = b2.x;
-            bv[2 * q + 1] = b2.y;
+    const int32_t r0 = r_s + blockIdx.y * GT, c0 = c_s + blockIdx.x * GT;
+    if (c0 > r0 + GT - 1) return;
+    double* As = dsm;                  // [2][GT][GP]
+    double* Bs = dsm + 2 * GT * GP;    // [2][GT][GP]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 2) * 64, wc = (warp & 3) * 32;  // warp tile origin in the CTA tile
+    const int fr = lane >> 2, fk = lane & 3;                // fragment row / k of this lane
+    auto load = [&](int buf, int kc) {
+        // 128 rows x 32 doubles = 2048 16-byte pieces per operand, 8 per thread
+        for (int idx = tid; idx < GT * (GK / 2); idx += 256) {
+            const int rr = idx / (GK / 2), pc = (idx % (GK / 2)) * 2;
+            const int32_t ra = min(r0 + rr, n - 1), rb = min(c0 + rr, n - 1);
+            cp_async16(As + (size_t)buf * GT * GP + rr * GP + pc, L + (int64_t)ra * n + k0 + kc + pc);
+            cp_async16(Bs + (size_t)buf * GT * GP + rr * GP + pc, L + (int64_t)rb * n + k0 + kc + pc);
         }
+        cp_async_commit();
+    };
+    double acc[8][4][2];
 #pragma unroll
-        for (int p = 0; p < 8; p++)
+    for (int i = 0; i < 8; i++)
 #pragma unroll
-            for (int q = 0; q < 8; q++) acc[p][q] = fma(av[p], bv[q], acc[p][q]);
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    const int nch = kl / GK;
+    load(0, 0);
+    for (int ch = 0; ch < nch; ch++) {
+        if (ch + 1 < nch) {
+            load((ch + 1) & 1, (ch + 1) * GK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double* Ab = As + (size_t)(ch & 1) * GT * GP + (wr + fr) * GP + fk;
+        const double* Bb = Bs + (size_t)(ch & 1) * GT * GP + (wc + fr) * GP + fk;
+#pragma unroll
+        for (int kk = 0; kk < GK; kk += 4) {
+            double af[8], bf[4];
+#pragma unroll
+            for (int i = 0; i < 8; i++) af[i] = Ab[i * 8 * GP + kk];
+#pragma unroll
+            for (int j = 0; j < 4; j++) bf[j] = Bb[j * 8 * GP + kk];
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+        __syncthreads();
     }
+    // accumulator (i, j): rows wr + 8i + lane/4, cols wc + 8j + 2(lane%4) + {0,1}
 #pragma unroll
-    for (int p = 0; p < 8; p++) {
-        const int32_t i = r0 + ty * 8 + p;
-        if (i >= n) continue;
-        double* row = L + (int64_t)i * n;
+    for (int i = 0; i < 8; i++) {
+        const int32_t row = r0 + wr + 8 * i + fr;
+        if (row >= n) continue;
+        double* rp = L + (int64_t)row * n;
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int32_t c = c0 + 32 * (q >> 1) + 2 * tx + (q & 1);
-            if (c < n && c <= i) row[c] -= acc[p][q];
+        for (int j = 0; j < 4; j++) {
+            const int32_t col = c0 + wc + 8 * j + 2 * fk;
+            if (col < c_e && col <= row) rp[col] -= acc[i][j][0];
+            if (col + 1 < c_e && col + 1 <= row) rp[col + 1] -= acc[i][j][1];
         }
     }
 }
 
-// ---- triangular solves: B[nrhs][n] ------------------------------------------
-
-// Triangular-solve block steps. Dynamic shared memory: the 64x64 diagonal
-// inverse, one 64x64 tile of L and the block of right-hand sides, all staged
-// with coalesced loads.
+// Triangular solves keep the 64x64 diagonal inverse, one 64x64 tile of L and
+// the block of right-hand sides in shared memory, staged with coalesced loads.
 constexpr int TP = NB + 1;
 
-// Forward step kb: y = inv(L_kk) b_kk (every CTA recomputes it from shared
-// memory), CTA 0 stores y into Y; CTA j updates the 64 rows after block kb it
-// owns: b_row -= L[row][kb block] y.
+// (L L^T) X = B in one cooperative launch. Forward: for each 64-block kb every
+// CTA recomputes y = inv(L_kk) b_kk in shared memory, CTA 0 stores it, and the
+// CTAs update the row blocks after kb that they own (block j belongs to CTA
+// (j - kb - 1) mod G); one grid barrier per block. Backward mirrors it with
+// inv(L_kk)^T and the column blocks before kb. B is overwritten with X; W is
+// scratch of the same shape. Requires all G CTAs resident (cooperative launch).
 __global__ void __launch_bounds__(256)
-trsv_fwd_kernel(const double* __restrict__ L, const double* __restrict__ Linv, int32_t n,
-                int32_t kb, double* __restrict__ B, double* __restrict__ Y, int32_t nrhs) {
+chol_solve_coop_kernel(const double* __restrict__ L, const double* __restrict__ Linv, int32_t n,
+                       double* __restrict__ B, double* __restrict__ W, int32_t nrhs) {
+    cg::grid_group grid = cg::this_grid();
     extern __shared__ double sm[];
-    double* li = sm;              // [NB][TP]
-    double* lt = li + NB * TP;    // [NB][TP]
-    double* bb = lt + NB * TP;    // [nrhs][NB]
-    double* y = bb + nrhs * NB;   // [nrhs][NB]
-    const int32_t r0 = kb * NB;
-    const int32_t s = min(NB, n - r0);
+    double* li = sm;                 // [NB][TP]
+    double* lt = li + NB * TP;       // [NB][TP]
+    double* yb = lt + NB * TP;       // [nrhs][NB]
+    double* y = yb + nrhs * NB;      // [nrhs][NB]
+    const int32_t nb = (n + NB - 1) / NB;
     const int tid = threadIdx.x;
-    const double* Li = Linv + (int64_t)kb * NB * NB;
-    for (int idx = tid; idx < NB * NB; idx += 256) li[(idx / NB) * TP + idx % NB] = Li[idx];
-    for (int idx = tid; idx < nrhs * NB; idx += 256) {
-        const int q = idx / NB, m = idx % NB;
-        bb[idx] = (m < s) ? B[(int64_t)q * n + r0 + m] : 0.0;
-    }
-    const int32_t row0 = r0 + NB + blockIdx.x * NB;
-    for (int idx = tid; idx < NB * NB; idx += 256) {
-        const int rr = idx / NB, m = idx % NB;
-        lt[rr * TP + m] = (row0 + rr < n && m < s) ? L[(int64_t)(row0 + rr) * n + r0 + m] : 0.0;
-    }
-    __syncthreads();
-    for (int idx = tid; idx < nrhs * NB; idx += 256) {
-        const int q = idx / NB, i = idx % NB;
-        double acc = 0.0;
-        for (int m = 0; m <= i; m++) acc += li[i * TP + m] * bb[q * NB + m];
-        y[idx] = acc;
-    }
-    __syncthreads();
-    if (blockIdx.x == 0)
+    const int G = gridDim.x;
+    // forward: W = inv(L) B
+    for (int32_t kb = 0; kb < nb; kb++) {
+        const int32_t r0 = kb * NB, s = min(NB, n - r0);
+        const double* Li = Linv + (int64_t)kb * NB * NB;
+        for (int idx = tid; idx < NB * NB; idx += 256) li[(idx / NB) * TP + idx % NB] = Li[idx];
+        for (int idx = tid; idx < nrhs * NB; idx += 256) {
+            const int q = idx / NB, m = idx % NB;
+            yb[idx] = (m < s) ? B[(int64_t)q * n + r0 + m] : 0.0;
+        }
+        __syncthreads();
         for (int idx = tid; idx < nrhs * NB; idx += 256) {
             const int q = idx / NB, i = idx % NB;
-            if (i < s) Y[(int64_t)q * n + r0 + i] = y[idx];
+            double acc = 0.0;
+            for (int m = 0; m <= i; m++) acc += li[i * TP + m] * yb[q * NB + m];
+            y[idx] = acc;
         }
-    if (row0 >= n) return;
-    for (int idx = tid; idx < nrhs * NB; idx += 256) {
-        const int q = idx / NB, rr = idx % NB;
-        if (row0 + rr >= n) continue;
-        double acc = 0.0;
+        __syncthreads();
+        if (blockIdx.x == 0)
+            for (int idx = tid; idx < nrhs * NB; idx += 256) {
+                const int q = idx / NB, i = idx % NB;
+                if (i < s) W[(int64_t)q * n + r0 + i] = y[idx];
+            }
+        for (int32_t jb = kb + 1 + blockIdx.x; jb < nb; jb += G) {
+            const int32_t row0 = jb * NB;
+            __syncthreads();
+            for (int idx = tid; idx < NB * NB; idx += 256) {
+                const int rr = idx / NB, m = idx % NB;
+                lt[rr * TP + m] = (row0 + rr < n && m < s) ? L[(int64_t)(row0 + rr) * n + r0 + m] : 0.0;
+            }
+            __syncthreads();
+            for (int idx = tid; idx < nrhs * NB; idx += 256) {
+                const int q = idx / NB, rr = idx % NB;
+                if (row0 + rr >= n) continue;
+                double acc = 0.0;
 #pragma unroll 8
-        for (int m = 0; m < NB; m++) acc += lt[rr * TP + m] * y[q * NB + m];
-        B[(int64_t)q * n + row0 + rr] -= acc;
-    }
-}
-
-// Backward step kb: x = inv(L_kk)^T y_kk, CTA 0 stores x into X; CTA j updates
-// the 64 columns it owns before block kb: y_c -= sum_r L[kb*64 + r][c] x_r.
-__global__ void __launch_bounds__(256)
-trsv_bwd_kernel(const double* __restrict__ L, const double* __restrict__ Linv, int32_t n,
-                int32_t kb, double* __restrict__ Yv, double* __restrict__ X, int32_t nrhs) {
-    extern __shared__ double sm[];
-    double* li = sm;
-    double* lt = li + NB * TP;
-    double* yb = lt + NB * TP;
-    double* x = yb + nrhs * NB;
-    const int32_t r0 = kb * NB;
-    const int32_t s = min(NB, n - r0);
-    const int tid = threadIdx.x;
-    const double* Li = Linv + (int64_t)kb * NB * NB;
-    for (int idx = tid; idx < NB * NB; idx += 256) li[(idx / NB) * TP + idx % NB] = Li[idx];
-    for (int idx = tid; idx < nrhs * NB; idx += 256) {
-        const int q = idx / NB, m = idx % NB;
-        yb[idx] = (m < s) ? Yv[(int64_t)q * n + r0 + m] : 0.0;
-    }
-    const int32_t col0 = blockIdx.x * NB;
-    const bool upd = col0 < r0;
-    if (upd)
-        for (int idx = tid; idx < NB * NB; idx += 256) {
-            const int r = idx / NB, cc = idx % NB;
-            lt[r * TP + cc] = (r < s) ? L[(int64_t)(r0 + r) * n + col0 + cc] : 0.0;
+                for (int m = 0; m < NB; m++) acc += lt[rr * TP + m] * y[q * NB + m];
+                B[(int64_t)q * n + row0 + rr] -= acc;
+            }
         }
-    __syncthreads();
-    for (int idx = tid; idx < nrhs * NB; idx += 256) {
-        const int q = idx / NB, i = idx % NB;
-        double acc = 0.0;
-        for (int m = i; m < NB; m++) acc += li[m * TP + i] * yb[q * NB + m];
-        x[idx] = acc;
+        grid.sync();
     }
-    __syncthreads();
-    if (blockIdx.x == 0)
+    // backward: B = inv(L)^T W
+    for (int32_t kb = nb - 1; kb >= 0; kb--) {
+        const int32_t r0 = kb * NB, s = min(NB, n - r0);
+        const double* Li = Linv + (int64_t)kb * NB * NB;
+        for (int idx = tid; idx < NB * NB; idx += 256) li[(idx / NB) * TP + idx % NB] = Li[idx];
+        for (int idx = tid; idx < nrhs * NB; idx += 256) {
+            const int q = idx / NB, m = idx % NB;
+            yb[idx] = (m < s) ? W[(int64_t)q * n + r0 + m] : 0.0;
+        }
+        __syncthreads();
         for (int idx = tid; idx < nrhs * NB; idx += 256) {
             const int q = idx / NB, i = idx % NB;
-            if (i < s) X[(int64_t)q * n + r0 + i] = x[idx];
+            double acc = 0.0;
+            for (int m = i; m < NB; m++) acc += li[m * TP + i] * yb[q * NB + m];
+            y[idx] = acc;
         }
-    if (!upd) return;
-    for (int idx = tid; idx < nrhs * NB; idx += 256) {
-        const int q = idx / NB, cc = idx % NB;
-        double acc = 0.0;
+        __syncthreads();
+        if (blockIdx.x == 0)
+            for (int idx = tid; idx < nrhs * NB; idx += 256) {
+                const int q = idx / NB, i = idx % NB;
+                if (i < s) B[(int64_t)q * n + r0 + i] = y[idx];
+            }
+        for (int32_t jb = blockIdx.x; jb < kb; jb += G) {
+            const int32_t col0 = jb * NB;
+            __syncthreads();
+            for (int idx = tid; idx < NB * NB; idx += 256) {
+                const int r = idx / NB, cc = idx % NB;
+                lt[r * TP + cc] = (r < s) ? L[(int64_t)(r0 + r) * n + col0 + cc] : 0.0;
+            }
+            __syncthreads();
+            for (int idx = tid; idx < nrhs * NB; idx += 256) {
+                const int q = idx / NB, cc = idx % NB;
+                double acc = 0.0;
 #pragma unroll 8
-        for (int r = 0; r < NB; r++) acc += lt[r * TP + cc] * x[q * NB + r];
-        Yv[(int64_t)q * n + col0 + cc] -= acc;
+                for (int r = 0; r < NB; r++) acc += lt[r * TP + cc] * y[q * NB + r];
+                W[(int64_t)q * n + col0 + cc] -= acc;
+            }
+        }
+        grid.sync();
     }
 }
 
@@ -464,33 +553,80 @@ inline int32_t grid_for(int64_t n, int bs) { return (int32_t)((n + bs - 1) / bs)
 
 int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, double piv_tol,
                       int32_t* singular) {
+    // Right-looking, outer panels of 256 columns, with look-ahead. On the main
+    // stream: each 64-column block of the panel is factored (potrf_diag), every
+    // row below it is solved against the block (trsm_panel: A_ik inv(L_kk)^T)
+    // and the rest of the panel gets the rank-64 update. On the second stream:
+    // the trailing matrix gets the rank-256 update, first the columns of the
+    // next panel (which the main stream waits for) and then the rest, which
+    // overlaps the next panel's factorization (disjoint columns).
     const int32_t nb = (n + NB - 1) / NB;
+    constexpr int32_t OUT = 4;  // 64-blocks per outer panel
+    const int32_t nsteps = (nb + OUT - 1) / OUT;
     TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
     int32_t* st = ctx->status.as<int32_t>();
     TPE_CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(int32_t), ctx->stream));
     const size_t sm1 = sizeof(double) * 2 * NB * (NB + 1);
-    const size_t sm2 = sizeof(double) * 2 * NB * SP;
-    TPE_CUDA_TRY(cudaFuncSetAttribute(potrf_diag_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    const size_t sm0 = sizeof(double) * 3 * NB * (NB + 1);
+    const size_t smg = sizeof(double) * 4 * GT * GP;
+    TPE_CUDA_TRY(cudaFuncSetAttribute(potrf_diag_kernel<double>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm0));
     TPE_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-    TPE_CUDA_TRY(cudaFuncSetAttribute(syrk_update_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-    KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 3 * (int64_t)nb - 2);
-    for (int32_t kb = 0; kb < nb; kb++) {
-        potrf_diag_kernel<<<1, 256, sm1, ctx->stream>>>(d_L, d_Linv, n, kb, piv_tol, st);
-        const int32_t rest = nb - kb - 1;
-        if (rest > 0) {
-            trsm_panel_kernel<<<rest, 256, sm1, ctx->stream>>>(d_L, d_Linv, n, kb);
-            const int64_t nt2 = ((int64_t)rest * NB + ST - 1) / ST;
-            const int64_t tiles = nt2 * (nt2 + 1) / 2;
-            syrk_update_kernel<<<(unsigned)tiles, 256, sm2, ctx->stream>>>(d_L, n, kb);
+    TPE_CUDA_TRY(cudaFuncSetAttribute(gemm_lower_update_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg));
+    while ((int32_t)ctx->fac_events.size() < 2 * nsteps + 2) {
+        cudaEvent_t e;
+        TPE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->fac_events.push_back(e);
+    }
+    cudaEvent_t* ev = ctx->fac_events.data();
+    int64_t launches = 0;
+    for (int32_t K0b = 0; K0b < nb; K0b += OUT) {
+        const int32_t kend = min(nb, K0b + OUT);
+        for (int32_t kb = K0b; kb < kend; kb++)
+            launches += 1 + (nb - kb - 1 > 0 ? 1 : 0) + (kb + 1 < kend ? 1 : 0);
+        launches += kend < nb ? 1 : 0;
+        launches += (kend + OUT) * NB < n ? 1 : 0;
+    }
+    KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, launches);
+    cudaStream_t sa = ctx->stream, sb = ctx->stream2;
+    // the second stream starts after everything already queued on the main one
+    TPE_CUDA_TRY(cudaEventRecord(ev[2 * nsteps], sa));
+    TPE_CUDA_TRY(cudaStreamWaitEvent(sb, ev[2 * nsteps], 0));
+    for (int32_t s = 0; s < nsteps; s++) {
+        const int32_t K0b = s * OUT, kend = min(nb, K0b + OUT);
+        if (s > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(sa, ev[2 * (s - 1) + 1], 0));
+        for (int32_t kb = K0b; kb < kend; kb++) {
+            potrf_diag_kernel<double><<<1, 256, sm0, sa>>>(d_L, d_Linv, n, kb, piv_tol, st);
+            const int32_t rest = nb - kb - 1;
+            if (rest > 0) trsm_panel_kernel<<<rest, 256, sm1, sa>>>(d_L, d_Linv, n, kb);
+            if (kb + 1 < kend) {
+                const int32_t r_s = (kb + 1) * NB, c_e = min(n, kend * NB);
+                dim3 g((c_e - r_s + GT - 1) / GT, (n - r_s + GT - 1) / GT);
+                gemm_lower_update_kernel<<<g, 256, smg, sa>>>(d_L, n, r_s, r_s, c_e, kb * NB, NB);
+            }
+        }
+        TPE_CUDA_TRY(cudaEventRecord(ev[2 * s], sa));
+        if (kend < nb) {
+            TPE_CUDA_TRY(cudaStreamWaitEvent(sb, ev[2 * s], 0));
+            const int32_t r_s = kend * NB, c_next = min(n, (kend + OUT) * NB);
+            const int32_t k0 = K0b * NB, kl = (kend - K0b) * NB;
+            dim3 g1((c_next - r_s + GT - 1) / GT, (n - r_s + GT - 1) / GT);
+            gemm_lower_update_kernel<<<g1, 256, smg, sb>>>(d_L, n, r_s, r_s, c_next, k0, kl);
+            TPE_CUDA_TRY(cudaEventRecord(ev[2 * s + 1], sb));
+            if (c_next < n) {
+                dim3 g2((n - c_next + GT - 1) / GT, (n - c_next + GT - 1) / GT);
+                gemm_lower_update_kernel<<<g2, 256, smg, sb>>>(d_L, n, c_next, c_next, n, k0, kl);
+            }
         }
     }
+    TPE_CUDA_TRY(cudaEventRecord(ev[2 * nsteps + 1], sb));
+    TPE_CUDA_TRY(cudaStreamWaitEvent(sa, ev[2 * nsteps + 1], 0));
     TPE_CUDA_TRY(cudaGetLastError());
     int32_t h = 0;
-    TPE_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    TPE_CUDA_TRY(cudaMemcpyAsync(&h, st, sizeof(int32_t), cudaMemcpyDeviceToHost, sa));
+    TPE_CUDA_TRY(cudaStreamSynchronize(sa));
     *singular = h;
     return TPE_OK;
 }
@@ -498,29 +634,30 @@ int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, doub
 int32_t chol_solve_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
                         double* d_B, int32_t nrhs) {
     if (nrhs <= 0) return TPE_OK;
-    const int32_t nb = (n + NB - 1) / NB;
-    TPE_TRY(ensure(ctx, ctx->solve_scratch, sizeof(double) * (size_t)n * nrhs));
-    double* Y = ctx->solve_scratch.as<double>();
-    const size_t smem = sizeof(double) * (2 * (size_t)NB * TP + 2 * (size_t)nrhs * NB);
     if (nrhs > 64) {
         set_error(ctx, TPE_ERR_TOO_LARGE, "chol_solve: at most 64 right-hand sides per call");
         return TPE_ERR_TOO_LARGE;
     }
-    TPE_CUDA_TRY(cudaFuncSetAttribute(trsv_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(double) * (2 * NB * TP + 2 * 64 * NB))));
-    TPE_CUDA_TRY(cudaFuncSetAttribute(trsv_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(double) * (2 * NB * TP + 2 * 64 * NB))));
-    KernelScope ks(ctx, TPE_KGROUP_TRSV, 2 * (int64_t)nb);
-    for (int32_t kb = 0; kb < nb; kb++) {
-        const int32_t rows_after = n - (kb + 1) * NB;
-        const int32_t g = rows_after > 0 ? (rows_after + NB - 1) / NB : 1;
-        trsv_fwd_kernel<<<g, 256, smem, ctx->stream>>>(d_L, d_Linv, n, kb, d_B, Y, nrhs);
+    const int32_t nb = (n + NB - 1) / NB;
+    TPE_TRY(ensure(ctx, ctx->solve_scratch, sizeof(double) * (size_t)n * nrhs));
+    double* W = ctx->solve_scratch.as<double>();
+    const size_t smem = sizeof(double) * (2 * (size_t)NB * TP + 2 * (size_t)nrhs * NB);
+    const int smax = (int)(sizeof(double) * (2 * NB * TP + 2 * 64 * NB));
+    TPE_CUDA_TRY(cudaFuncSetAttribute(chol_solve_coop_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+    int per_sm = 0;
+    TPE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chol_solve_coop_kernel, 256,
+                                                               smem));
+    int G = per_sm * ctx->num_sms;
+    if (G > nb) G = nb;
+    if (G < 1) {
+        set_error(ctx, TPE_ERR_CUDA, "chol_solve: cooperative kernel does not fit on an SM");
+        return TPE_ERR_CUDA;
     }
-    for (int32_t kb = nb - 1; kb >= 0; kb--) {
-        const int32_t g = kb > 0 ? kb : 1;
-        trsv_bwd_kernel<<<g, 256, smem, ctx->stream>>>(d_L, d_Linv, n, kb, Y, d_B, nrhs);
-    }
-    TPE_CUDA_TRY(cudaGetLastError());
+    KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
+    void* args[] = {(void*)&d_L, (void*)&d_Linv, (void*)&n, (void*)&d_B, (void*)&W, (void*)&nrhs};
+    TPE_CUDA_TRY(cudaLaunchCooperativeKernel((void*)chol_solve_coop_kernel, dim3(G), dim3(256), args,
+                                             smem, ctx->stream));
     return TPE_OK;
 }
 

@@ -333,6 +333,24 @@ inline int32_t pick_chunks(const tpe_ctx* ctx, int32_t E, int32_t ncurves) {
 
 }  // namespace
 
+int32_t reduce_partials_launch(tpe_ctx* ctx, const double* partial, int32_t nparts, int32_t ncurves,
+                               double scale, double* out) {
+    KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+    reduce_partials<<<ncurves, 256, 0, ctx->stream>>>(partial, nparts, scale, out);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
+int32_t gather_vertex_grad_launch(tpe_ctx* ctx, const double* edge_acc, int32_t nchunks,
+                                  double* grad) {
+    KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+    gather_vertex_grad<<<(ctx->V + 127) / 128, 128, 0, ctx->stream>>>(
+        edge_acc, nchunks, ctx->E, ctx->d_inc_off.as<int32_t>(), ctx->d_inc.as<int32_t>(), ctx->V,
+        grad);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
 int32_t edge_prep(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps,
                   double alpha) {
     const int32_t E = ctx->E;

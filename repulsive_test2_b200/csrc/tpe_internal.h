@@ -75,6 +75,8 @@ struct DevBlock {
 struct tpe_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;           // look-ahead stream of the factorization
+    std::vector<cudaEvent_t> fac_events;      // dependency events (no timing)
     std::string err;
     int32_t num_sms = 0;
 
@@ -90,6 +92,7 @@ struct tpe_ctx {
     tpe::DevBuf pos, pos2, pos3, edge_a, edge_b, grad, edge_acc, partial, scalars, flat0, flat1,
         flat2, flat3, dir;
     tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
+    tpe::DevBuf edge_m;                     // mixed-precision edge records (4 float4 per edge)
     tpe::DevBuf mat_A, mat_L, mat_Linv, mat_B, mat_B0;
     tpe::DevBuf con_C, con_Y, con_phi, con_blocks, con_ell0, con_red;
     tpe::DevBuf rhs, sol, tmp, solve_scratch;
@@ -141,6 +144,15 @@ int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2
 // Energy (optional) and gradient (interleaved V x 3) of one curve.
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
                          double* d_grad);
+
+// ---- mixed precision pair kernels (pair_mixed.cu) ----------------------------
+int32_t edge_prep_mixed(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps,
+                        double alpha);
+int32_t energy_mixed(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, double eps,
+                     double* d_energy);
+int32_t energy_grad_mixed(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
+                          double* d_grad);
+int32_t assemble_mixed(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_A);
 
 // ---- assembly (assembly.cu) -----------------------------------------------
 // A (and optionally B, B0) V x V row-major FP64 from prepared edge records.
