@@ -124,7 +124,9 @@ typedef struct {
     int32_t converged;
     int32_t projection_iterations; /* -1 = null */
     int32_t reason;                /* TPE_REASON_* */
-    int32_t refine_iterations;     /* mixed path */
+    int32_t refine_iterations;     /* mixed path: CG iterations of the gradient solve;
+                                      0 = FP64 factorization, -1 = mixed requested but the
+                                      FP32 factor broke down or CG missed refine_tol (FP64 used) */
     int32_t trials_evaluated;      /* tau trials whose energy was evaluated */
 } tpe_step_stats;
 

@@ -334,6 +334,10 @@ def _opts(o: Optional[Dict[str, Any]] = None, **kw) -> abi.tpe_step_opts:
         op.proj_max_iter = int(proj["maxIter"])
     if d.get("precision") == "mixed":
         op.precision = abi.PRECISION_MIXED
+    if d.get("refineTol") is not None:
+        op.refine_tol = float(d["refineTol"])
+    if d.get("refineMaxIter") is not None:
+        op.refine_max_iter = int(d["refineMaxIter"])
     if d.get("trials"):
         op.trials = int(d["trials"])
     if d.get("collectField"):
@@ -384,6 +388,8 @@ def _stats_dict(st: abi.tpe_step_stats) -> Dict[str, Any]:
         "gradientL2Norm": st.gradient_l2_norm,
         "projectionIterations": None if st.projection_iterations < 0 else st.projection_iterations,
         **({"reason": abi.REASONS[st.reason]} if st.reason else {}),
+        # extension: CG iterations of the mixed-precision solve (0 = FP64, -1 = FP64 fallback)
+        "refineIterations": st.refine_iterations,
     }
 
 

@@ -291,9 +291,14 @@ int32_t check_topology(tpe_ctx* ctx) {
 // Factor A_rho and the Schur complement from ctx->mat_A (V x V) and ctx->con_C (k x 3V).
 // *singular set when the reference would report a singular system.
 int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
-                    const double* b_flat = nullptr) {
+                    const double* b_flat = nullptr, const tpe_step_opts* o = nullptr) {
     SaddleOp& op = ctx->op;
     op.valid = false;
+    op.mixed = false;
+    op.mixed_fallback = false;
+    op.refine_iters = 0;
+    op.refine_max_iter = o ? o->refine_max_iter : 30;
+    op.refine_tol = o ? o->refine_tol : 1e-12;
     op.V = V;
     op.k = k;
     op.A = ctx->mat_A.as<double>();
@@ -330,34 +335,60 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
         *singular = true;
         return TPE_OK;
     }
-    TPE_TRY(shift_copy(ctx, op.A, op.L, V, rho / V));
-    int32_t bad = 0;
-    const double tol = 32.0 * 2.220446049250313e-16 * (tm[1] + rho / V);
-    TPE_TRY(cholesky_fp64(ctx, op.L, op.Linv, V, tol, &bad));
-    if (bad) {
-        *singular = true;
-        return TPE_OK;
-    }
     op.Scc.assign((size_t)k * k, 0.0);
     op.Scu.assign((size_t)k * 3, 0.0);
     op.trans_constrained = false;
-    // One triangular solve for Y = Abar_rho^{-1} C^T (3k right-hand sides of
-    // length V) and, when given, w = Abar_rho^{-1} b (3 more), in groups of 64.
-    {
-        const int32_t rows = k + (b_flat ? 1 : 0);
-        TPE_TRY(ensure(ctx, ctx->con_Y, sizeof(double) * (size_t)(rows > 0 ? rows : 1) * 3 * V));
-        op.Y = ctx->con_Y.as<double>();
-        if (k > 0)
-            TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
-                                         cudaMemcpyDeviceToDevice, ctx->stream));
-        if (b_flat) {
-            op.W = op.Y + (size_t)k * 3 * V;
-            op.w_src = b_flat;
-            TPE_CUDA_TRY(cudaMemcpyAsync(op.W, b_flat, sizeof(double) * 3 * (size_t)V,
-                                         cudaMemcpyDeviceToDevice, ctx->stream));
+    // Y = Abar_rho^{-1} C^T (3k right-hand sides of length V) and, when given,
+    // w = Abar_rho^{-1} b (3 more), solved together.
+    const int32_t rows = k + (b_flat ? 1 : 0);
+    TPE_TRY(ensure(ctx, ctx->con_Y, sizeof(double) * (size_t)(rows > 0 ? rows : 1) * 3 * V));
+    op.Y = ctx->con_Y.as<double>();
+    if (k > 0)
+        TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+    if (b_flat) {
+        op.W = op.Y + (size_t)k * 3 * V;
+        op.w_src = b_flat;
+        TPE_CUDA_TRY(cudaMemcpyAsync(op.W, b_flat, sizeof(double) * 3 * (size_t)V,
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    const int32_t nrhs = 3 * rows;
+    if (o && o->precision == TPE_PRECISION_MIXED && nrhs <= kMixedMaxRhs) {
+        // FP32 tensor-core factor as the preconditioner of an FP64 CG; the FP64
+        // factorization below is the fallback (breakdown or no convergence).
+        bool ok = false;
+        TPE_TRY(mixed_factor(ctx, op.A, V, rho, &ok));
+        if (ok && nrhs > 0) {
+            bool conv = false;
+            int32_t it = 0;
+            TPE_TRY(mixed_solve(ctx, op.A, op.Y, op.Y, nrhs, o->refine_max_iter, o->refine_tol,
+                                &it, &conv));
+            op.refine_iters = it;
+            ok = conv;
         }
-        for (int32_t r0 = 0; r0 < 3 * rows; r0 += 64) {
-            const int32_t nr = (3 * rows - r0) < 64 ? (3 * rows - r0) : 64;
+        if (ok) {
+            op.mixed = true;
+        } else {
+            op.mixed_fallback = true;
+            if (k > 0)
+                TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
+                                             cudaMemcpyDeviceToDevice, ctx->stream));
+            if (b_flat)
+                TPE_CUDA_TRY(cudaMemcpyAsync(op.W, b_flat, sizeof(double) * 3 * (size_t)V,
+                                             cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+    }
+    if (!op.mixed) {
+        TPE_TRY(shift_copy(ctx, op.A, op.L, V, rho / V));
+        int32_t bad = 0;
+        const double tol = 32.0 * 2.220446049250313e-16 * (tm[1] + rho / V);
+        TPE_TRY(cholesky_fp64(ctx, op.L, op.Linv, V, tol, &bad));
+        if (bad) {
+            *singular = true;
+            return TPE_OK;
+        }
+        for (int32_t r0 = 0; r0 < nrhs; r0 += 64) {
+            const int32_t nr = (nrhs - r0) < 64 ? (nrhs - r0) : 64;
             TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, op.Y + (size_t)r0 * V, nr));
         }
     }
@@ -426,26 +457,23 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
 }
 
 // Assemble A and C at device positions d_pos (set already uploaded) and factor.
+// A is assembled in FP64 in every precision mode: rounding its entries to FP32
+// moves the Sobolev gradient by far more than the mixed mode's tolerance.
 int32_t op_build(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k, double alpha,
                  double beta, double eps, bool* singular, double* timings,
-                 const double* b_flat = nullptr, int32_t precision = TPE_PRECISION_FP64) {
+                 const double* b_flat = nullptr, const tpe_step_opts* o = nullptr) {
     const int32_t V = ctx->V;
     {
         Timer t(ctx, timings, TPE_PHASE_ASSEMBLEA);
         TPE_TRY(ensure(ctx, ctx->mat_A, sizeof(double) * (size_t)V * V));
-        if (precision == TPE_PRECISION_MIXED) {
-            TPE_TRY(edge_prep_mixed(ctx, d_pos, 1, eps, alpha));
-            TPE_TRY(assemble_mixed(ctx, alpha, beta, eps, ctx->mat_A.as<double>()));
-        } else {
-            TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
-            TPE_TRY(assemble_fp64(ctx, alpha, beta, eps, ctx->mat_A.as<double>(), nullptr, nullptr));
-        }
+        TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
+        TPE_TRY(assemble_fp64(ctx, alpha, beta, eps, ctx->mat_A.as<double>(), nullptr, nullptr));
     }
     TPE_TRY(ensure(ctx, ctx->con_C, sizeof(double) * (size_t)(k > 0 ? k : 1) * 3 * V));
     std::vector<double> phi, ns;
     TPE_TRY(eval_constraints(ctx, d_pos, nblocks, k, ctx->con_C.as<double>(), phi, ns));
     Timer t(ctx, timings, TPE_PHASE_FACTOR);
-    return op_finalize(ctx, V, k, singular, b_flat);
+    return op_finalize(ctx, V, k, singular, b_flat, o);
 }
 
 // Solve with the current operator: b_flat (device, 3V, or null = 0), d (host, k,
@@ -464,7 +492,19 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
         } else {
             TPE_CUDA_TRY(cudaMemcpyAsync(w, b_flat, sizeof(double) * m, cudaMemcpyDeviceToDevice,
                                          ctx->stream));
-            TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, w, 3));
+            if (op.mixed) {
+                bool conv = false;
+                int32_t it = 0;
+                TPE_TRY(mixed_solve(ctx, op.A, w, w, 3, op.refine_max_iter, op.refine_tol, &it,
+                                    &conv));
+                if (!conv) {
+                    set_error(ctx, TPE_ERR_REFINE_NOT_CONVERGED,
+                              "mixed-precision solve did not converge");
+                    return TPE_ERR_REFINE_NOT_CONVERGED;
+                }
+            } else {
+                TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, w, 3));
+            }
         }
         if (k > 0) {
             TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * ((size_t)k + 16)));
@@ -544,7 +584,7 @@ int32_t objective(tpe_ctx* ctx, const double* d_pos, const tpe_step_opts* o, boo
     double e = 0.0;
     {
         Timer t(ctx, timings, TPE_PHASE_ENERGY);
-        TPE_TRY(energy_of(ctx, d_pos, o->alpha, o->beta, o->epsilon, &e, o->precision));
+        TPE_TRY(energy_of(ctx, d_pos, o->alpha, o->beta, o->epsilon, &e));
     }
     if (pen) {
         double pe = 0.0;
@@ -638,7 +678,7 @@ int32_t project_dev(tpe_ctx* ctx, const double* d_start, const SetInfo& S, const
         if (!frozen) {
             bool singular = false;
             TPE_TRY(op_build(ctx, d_cur, S.nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular,
-                             timings, nullptr, o->precision));
+                             timings, nullptr, o));
             if (singular) {
                 *iters = it;
                 break;
@@ -1180,9 +1220,6 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
         Timer t(ctx, timings, TPE_PHASE_DE);
         if (o->mode == TPE_DE_FINITE_DIFF) {
             TPE_TRY(gradient_fd_dev(ctx, P, o->alpha, o->beta, o->epsilon, o->h, dE));
-        } else if (o->precision == TPE_PRECISION_MIXED) {
-            TPE_TRY(edge_prep_mixed(ctx, P, 1, o->epsilon, o->alpha));
-            TPE_TRY(energy_grad_mixed(ctx, o->alpha, o->beta, o->epsilon, nullptr, dE));
         } else {
             TPE_TRY(edge_prep(ctx, P, 1, o->epsilon, o->alpha));
             TPE_TRY(energy_grad_fp64(ctx, o->alpha, o->beta, o->epsilon, nullptr, dE));
@@ -1193,7 +1230,8 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
     TPE_TRY(interleaved_to_block(ctx, dE, ctx->flat2.as<double>(), V));
     bool singular = false;
     TPE_TRY(op_build(ctx, P, nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular, timings,
-                     ctx->flat2.as<double>(), o->precision));
+                     ctx->flat2.as<double>(), o));
+    st->refine_iterations = ctx->op.mixed ? ctx->op.refine_iters : (ctx->op.mixed_fallback ? -1 : 0);
     TPE_TRY(ensure(ctx, ctx->sol, sizeof(double) * m));
     double* out = ctx->sol.as<double>();
     if (singular) {

@@ -1,0 +1,850 @@
+// Mixed-precision saddle solve: the factorization of A_rho runs on the tensor
+// cores in FP32, the solution is made FP64-accurate by preconditioned CG.
+//
+// The FP64 path factors A_rho = A + (rho/V) 1 1^T (dense.cu) and back-substitutes.
+// Here the same SPD matrix is
+//   1. Jacobi-scaled, S = D A_rho D with D = diag(A_rho)^(-1/2), and rounded
+//      to FP32 (padded to Vp = 128 * 2^k rows with an identity block);
+//   2. factored S ~ L L^T in FP32: 128 x 128 diagonal blocks in one CTA
+//      (potrf128_kernel, which also inverts them), the panel solve and the
+//      trailing update as 3xTF32 tcgen05 GEMMs (tc_gemm.cu);
+//   3. inverted, Z = L^{-1}, by the recursive block formula
+//      Z21 = -Z22 L21 Z11, level by level with all blocks of a level batched
+//      into one tcgen05 GEMM; W = Z^T is kept beside Z so every product is an
+//      A * B^T of row-major operands;
+//   4. used as the preconditioner M = Z^T Z = (L L^T)^{-1} of a block CG on
+//      S y = D b in FP64, x = D y. Z and W are copied to FP64 once (hi + lo is
+//      exact) and every product of the CG -- S p with the FP64 A, Z r, W u --
+//      runs on the FP64 tensor cores (mrhs_dmma_kernel).
+// At V=8192 (kappa(A_rho) ~ 1e10, kappa(S) ~ 1e8) plain iterative refinement
+// with an FP32 factor diverges (kappa(S) * u32 > 1); CG with it reaches a 1e-13
+// relative residual in about 7 iterations. The FP64 path remains the fallback
+// whenever the FP32 factorization breaks down or CG does not converge.
+#include <math.h>
+
+#include "tc.h"
+#include "tpe_internal.h"
+
+namespace tpe {
+namespace {
+
+constexpr int kT = 128;       // diagonal block = GEMM tile
+constexpr int kLd = kT + 1;   // shared-memory row stride of a block (floats)
+constexpr int kMaxRhs = 16;   // right-hand sides per CG pass
+
+__host__ __device__ __forceinline__ void split32(float x, float& hi, float& lo) {
+    union {
+        float f;
+        uint32_t u;
+    } v;
+    v.f = x;
+    v.u = (v.u + 0x1000u) & 0xFFFFE000u;
+    hi = v.f;
+    lo = x - hi;
+}
+
+// d_i = 1 / sqrt(A_ii + shift) and dinv_i = 1 / d_i for real rows, 1 on the pad.
+__global__ void jacobi_kernel(const double* __restrict__ A, int32_t V, int32_t Vp, double shift,
+                              double* __restrict__ d, double* __restrict__ dinv) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Vp) return;
+    const double s = i < V ? sqrt(A[(size_t)i * V + i] + shift) : 1.0;
+    d[i] = 1.0 / s;
+    dinv[i] = s;
+}
+
+// S (Vp x Vp, FP32, ld Vp) = D (A + shift) D, identity on the pad.
+__global__ void scale_to_f32_kernel(const double* __restrict__ A, int32_t V, int32_t Vp,
+                                    double shift, const double* __restrict__ d,
+                                    float* __restrict__ S) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)Vp * Vp) return;
+    const int32_t i = (int32_t)(t / Vp), j = (int32_t)(t % Vp);
+    float v;
+    if (i < V && j < V)
+        v = (float)(d[i] * (A[(size_t)i * V + j] + shift) * d[j]);
+    else
+        v = (i == j) ? 1.0f : 0.0f;
+    S[t] = v;
+}
+
+// L[r0+i][c0+j] = split(S[r0+i][c0+j]) for i < rows, j < 128 (ld shared).
+__global__ void split_copy_kernel(const float* __restrict__ S, int32_t ld, int32_t r0, int32_t c0,
+                                  int32_t rows, float* __restrict__ hi, float* __restrict__ lo) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)rows * kT) return;
+    const size_t o = (size_t)(r0 + t / kT) * ld + c0 + (t % kT);
+    float h, l;
+    split32(S[o], h, l);
+    hi[o] = h;
+    lo[o] = l;
+}
+
+constexpr int kPw = 32;        // panel width inside a diagonal block
+constexpr int kPl = kPw + 1;   // row stride of the panel scratch
+
+// Column K of the in-register Cholesky of a 32 x 32 block (lane = row):
+// pivot from lane K, scale column K, update the columns right of it; the
+// template recursion keeps every register index static.
+template <int K>
+__device__ __forceinline__ void chol_col(float (&v)[32], int lane, bool& brk, float& myrs) {
+    if constexpr (K < 32) {
+        float piv = __shfl_sync(0xffffffffu, v[K], K);
+        if (!(piv > 0.0f) || !isfinite(piv)) {
+            brk = true;
+            piv = 1.0f;
+        }
+        const float rs = rsqrtf(piv);
+        if (lane == K) {
+            v[K] = piv * rs;
+            myrs = rs;
+        } else {
+            v[K] *= rs;
+        }
+        const float lk = v[K];
+#pragma unroll
+        for (int m = K + 1; m < 32; m++) {
+            const float lmk = __shfl_sync(0xffffffffu, v[K], m);
+            if (lane >= m) v[m] -= lk * lmk;
+        }
+        chol_col<K + 1>(v, lane, brk, myrs);
+    }
+}
+
+// Decodes the packed lower-triangular index e into (ti, tj), tj <= ti.
+__device__ __forceinline__ void tri_decode(int e, int& ti, int& tj) {
+    int t = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+    while ((t + 1) * (t + 2) / 2 <= e) t++;
+    while (t * (t + 1) / 2 > e) t--;
+    ti = t;
+    tj = e - t * (t + 1) / 2;
+}
+
+// One CTA factors the 128 x 128 diagonal block at (j0, j0) of S (lower
+// triangle read) and writes L_jj (split, zero above the diagonal) to L,
+// Z_jj = L_jj^{-1} (split, lower) to Z and W_jj = Z_jj^T (split, upper) to W.
+//
+// Blocked right-looking over four 32-column panels. Warp 0 factors a panel's
+// 32 x 32 diagonal part in registers (lane = row, column values shared by
+// shuffles, no block barriers) and inverts it by forward substitution (lane =
+// column of the inverse). All eight warps then solve the rows below against
+// that inverse (warp = 4 columns, lane = row) and apply the rank-32 update to
+// the lower trailing triangle in 4 x 4 register tiles. The off-diagonal
+// 32 x 32 blocks of the inverse follow from Z_ab = -Z_aa sum_{b<=c<a} L_ac Z_cb,
+// one block distance at a time, in the same 4 x 4 tiling. Reciprocal square
+// roots are the fast approximate ones: the factor is a preconditioner, CG
+// restores FP64 accuracy. *bad = 1 when a pivot is not positive and finite.
+__global__ void __launch_bounds__(256, 1)
+potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __restrict__ Lhi,
+                float* __restrict__ Llo, float* __restrict__ Zhi, float* __restrict__ Zlo,
+                float* __restrict__ Whi, float* __restrict__ Wlo, int32_t* __restrict__ bad) {
+    extern __shared__ float sm[];
+    float* a = sm;                  // the block, then L (lower)
+    float* z = a + kT * kLd;        // L^{-1} (lower)
+    float* pl = z + kT * kLd;       // 96 x 33 panel rows / block products
+    float* rd = pl + 96 * kPl;      // 1 / L_ii
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < kT * kT; e += 256) {
+        const int r = e >> 7, c = e & (kT - 1);
+        a[r * kLd + c] = (c <= r) ? S[(size_t)(j0 + r) * ld + j0 + c] : 0.0f;
+        z[r * kLd + c] = 0.0f;
+    }
+    __syncthreads();
+    for (int p = 0; p < kT / kPw; p++) {
+        const int c0 = p * kPw;
+        if (warp == 0) {
+            float v[kPw];
+#pragma unroll
+            for (int m = 0; m < kPw; m++) v[m] = (m <= lane) ? a[(c0 + lane) * kLd + c0 + m] : 0.0f;
+            bool brk = false;
+            float myrs = 1.0f;
+            chol_col<0>(v, lane, brk, myrs);
+            if (brk && lane == 0) atomicExch(bad, 1);
+#pragma unroll
+            for (int m = 0; m < kPw; m++) a[(c0 + lane) * kLd + c0 + m] = (m <= lane) ? v[m] : 0.0f;
+            rd[c0 + lane] = myrs;
+            __syncwarp();
+            // column `lane` of the inverse: forward substitution, axpy form
+            float x[kPw];
+#pragma unroll
+            for (int i = 0; i < kPw; i++) x[i] = (i == lane) ? 1.0f : 0.0f;
+#pragma unroll
+            for (int k = 0; k < kPw; k++) {
+                x[k] *= rd[c0 + k];
+#pragma unroll
+                for (int i = k + 1; i < kPw; i++) x[i] -= a[(c0 + i) * kLd + c0 + k] * x[k];
+            }
+#pragma unroll
+            for (int i = 0; i < kPw; i++) z[(c0 + i) * kLd + c0 + lane] = (i >= lane) ? x[i] : 0.0f;
+        }
+        __syncthreads();
+        const int nr = kT - c0 - kPw;
+        if (nr == 0) break;
+        // panel rows below: pl[r][m] = sum_k A[c0+32+r][c0+k] * Zd[m][k]
+        {
+            const int m0 = 4 * warp;
+            for (int r0 = 0; r0 < nr; r0 += 32) {
+                const int r = r0 + lane;
+                const float* arow = a + (c0 + kPw + r) * kLd + c0;
+                float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 8
+                for (int k = 0; k < kPw; k++) {
+                    const float ak = arow[k];
+#pragma unroll
+                    for (int t = 0; t < 4; t++) acc[t] += ak * z[(c0 + m0 + t) * kLd + c0 + k];
+                }
+#pragma unroll
+                for (int t = 0; t < 4; t++) pl[r * kPl + m0 + t] = acc[t];
+            }
+        }
+        __syncthreads();
+        // rank-32 update of the lower trailing triangle, 4 x 4 tiles
+        {
+            const int nt = nr / 4;
+            const int ntiles = nt * (nt + 1) / 2;
+            for (int e = tid; e < ntiles; e += 256) {
+                int ti, tj;
+                tri_decode(e, ti, tj);
+                float acc[4][4];
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+#pragma unroll
+                    for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+#pragma unroll 4
+                for (int k = 0; k < kPw; k++) {
+                    float pr[4], pc[4];
+#pragma unroll
+                    for (int x = 0; x < 4; x++) {
+                        pr[x] = pl[(4 * ti + x) * kPl + k];
+                        pc[x] = pl[(4 * tj + x) * kPl + k];
+                    }
+#pragma unroll
+                    for (int x = 0; x < 4; x++)
+#pragma unroll
+                        for (int y = 0; y < 4; y++) acc[x][y] += pr[x] * pc[y];
+                }
+                const int R = c0 + kPw + 4 * ti, Cc = c0 + kPw + 4 * tj;
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+#pragma unroll
+                    for (int y = 0; y < 4; y++) a[(R + x) * kLd + Cc + y] -= acc[x][y];
+            }
+        }
+        // the panel rows become final L
+        for (int e = tid; e < nr * kPw; e += 256) {
+            const int r = e >> 5, m = e & 31;
+            a[(c0 + kPw + r) * kLd + c0 + m] = pl[r * kPl + m];
+        }
+        __syncthreads();
+    }
+    // off-diagonal blocks of Z: T = sum_{c=b}^{a-1} L_ac Z_cb, then Z_ab = -Z_aa T
+    for (int d = 1; d < kT / kPw; d++) {
+        const int nbk = kT / kPw - d;
+        const int ntl = nbk * 64;  // 4 x 4 tiles of the nbk output blocks
+        float acc[4][4];
+        int bb = 0, tr = 0, tc = 0;
+        const bool act = tid < ntl;
+        if (act) {
+            bb = tid >> 6;
+            tr = (tid >> 3) & 7;
+            tc = tid & 7;
+        }
+        const int bi = bb + d, bj = bb;
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+        if (act) {
+            for (int k = bj * kPw; k < bi * kPw; k++) {
+                float lr[4], zc[4];
+#pragma unroll
+                for (int x = 0; x < 4; x++) {
+                    lr[x] = a[(bi * kPw + 4 * tr + x) * kLd + k];
+                    zc[x] = z[k * kLd + bj * kPw + 4 * tc + x];
+                }
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+#pragma unroll
+                    for (int y = 0; y < 4; y++) acc[x][y] += lr[x] * zc[y];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) pl[(bb * kPw + 4 * tr + x) * kPl + 4 * tc + y] = acc[x][y];
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+            const int rmax = 4 * tr + 3;
+            for (int q = 0; q <= rmax; q++) {
+                float zr[4], tq[4];
+#pragma unroll
+                for (int x = 0; x < 4; x++) {
+                    zr[x] = z[(bi * kPw + 4 * tr + x) * kLd + bi * kPw + q];
+                    tq[x] = pl[(bb * kPw + q) * kPl + 4 * tc + x];
+                }
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+#pragma unroll
+                    for (int y = 0; y < 4; y++) acc[x][y] += zr[x] * tq[y];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++)
+                    z[(bi * kPw + 4 * tr + x) * kLd + bj * kPw + 4 * tc + y] = -acc[x][y];
+        }
+        __syncthreads();
+    }
+    // stores: lane = column (coalesced rows, conflict-free shared reads)
+    for (int e = tid; e < kT * kT; e += 256) {
+        const int r = e >> 7, c = e & (kT - 1);
+        const size_t o = (size_t)(j0 + r) * ld + j0 + c;
+        float h, l;
+        split32(c <= r ? a[r * kLd + c] : 0.0f, h, l);
+        Lhi[o] = h;
+        Llo[o] = l;
+        split32(c <= r ? z[r * kLd + c] : 0.0f, h, l);
+        Zhi[o] = h;
+        Zlo[o] = l;
+        split32(r <= c ? z[c * kLd + r] : 0.0f, h, l);
+        Whi[o] = h;
+        Wlo[o] = l;
+    }
+}
+
+// W[s + c][s + m + r] = Z[s + m + r][s + c] (r, c < m), s = blockIdx.z * 2m.
+__global__ void transpose_block_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
+                                       float* __restrict__ whi, float* __restrict__ wlo,
+                                       int32_t ld, int32_t m) {
+    __shared__ float th[32][33], tl[32][33];
+    const int32_t s = blockIdx.z * 2 * m;
+    const int32_t r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const size_t o = (size_t)(s + m + r0 + yy) * ld + s + c0 + threadIdx.x;
+        th[yy][threadIdx.x] = zhi[o];
+        tl[yy][threadIdx.x] = zlo[o];
+    }
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const size_t o = (size_t)(s + c0 + yy) * ld + s + m + r0 + threadIdx.x;
+        whi[o] = th[threadIdx.x][yy];
+        wlo[o] = tl[threadIdx.x][yy];
+    }
+}
+
+// ---- block CG kernels (vectors are [nr][Vp] FP64, pad entries stay 0) ------
+
+// U = D P, s[c] = sum_j U[c][j]   (one block per column)
+__global__ void cg_prep_kernel(const double* __restrict__ P, const double* __restrict__ d,
+                               int32_t V, int32_t Vp, double* __restrict__ U,
+                               double* __restrict__ s) {
+    __shared__ double red[8];
+    const int c = blockIdx.x;
+    double acc = 0.0;
+    for (int32_t j = threadIdx.x; j < V; j += blockDim.x) {
+        const double u = d[j] * P[(size_t)c * Vp + j];
+        U[(size_t)c * Vp + j] = u;
+        acc += u;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        s[c] = t;
+    }
+}
+
+// ---- multi-right-hand-side products on the FP64 tensor cores ----------------
+//
+// part[z][c][i] = sum_{j in range z of row block} M[i][j] X[c][j] for c < 16:
+// mma.sync m8n8k4 (FP64), 64 rows per CTA (8 per warp), the row block's column
+// range split into gridDim.y equal parts (split K, summed in a fixed order by
+// mrhs_reduce_kernel). TRI = 0: all columns; 1: j < r0 + 64 (lower-triangular
+// M); 2: j >= r0 (upper). The K order inside a 16-column group is permuted
+// (MMA step s takes columns 4m + s, m = 0..3) so each lane's four consecutive
+// columns of M feed four MMAs without shuffles; X is staged transposed in
+// shared memory with rows padded to 17 doubles (conflict-free fragment loads).
+constexpr int kMvRows = 64;
+constexpr int kMvChunk = 256;
+constexpr int kXs = kMaxRhs + 1;
+
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <int TRI>
+__global__ void __launch_bounds__(256)
+mrhs_dmma_kernel(const double* __restrict__ M, int32_t ldm, int32_t n,
+                 const double* __restrict__ X, int32_t ldx, int32_t nr,
+                 double* __restrict__ part) {
+    __shared__ double xs[kMvChunk * kXs];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int32_t r0 = blockIdx.x * kMvRows;
+    int32_t lo = 0, hi = n;
+    if (TRI == 1) hi = min(n, r0 + kMvRows);
+    if (TRI == 2) lo = r0;
+    const int32_t per = (((hi - lo) + (int32_t)gridDim.y - 1) / (int32_t)gridDim.y + 15) / 16 * 16;
+    const int32_t ks = lo + (int32_t)blockIdx.y * per;
+    const int32_t ke = min(hi, ks + per);
+    const int32_t row = r0 + warp * 8 + (lane >> 2);
+    const bool rin = row < n;
+    const double* mrow = M + (size_t)(rin ? row : 0) * ldm;
+    const int m4 = (lane & 3) * 4;
+    const int gq = lane >> 2;
+    const bool vec = (ldm & 1) == 0;
+    double c0a = 0.0, c0b = 0.0, c1a = 0.0, c1b = 0.0;
+    for (int32_t kc = ks; kc < ke; kc += kMvChunk) {
+        const int32_t kn = min(kMvChunk, ke - kc);
+        __syncthreads();
+        for (int e = threadIdx.x; e < kMaxRhs * kMvChunk; e += 256) {
+            const int c = e / kMvChunk, jj = e % kMvChunk;
+            xs[jj * kXs + c] = (c < nr && jj < kn) ? X[(size_t)c * ldx + kc + jj] : 0.0;
+        }
+        __syncthreads();
+        for (int g = 0; g < kn; g += 16) {
+            const int32_t col = kc + g + m4;
+            double a[4];
+            if (rin && vec && col + 3 < ke) {
+                const double2 p0 = *reinterpret_cast<const double2*>(mrow + col);
+                const double2 p1 = *reinterpret_cast<const double2*>(mrow + col + 2);
+                a[0] = p0.x;
+                a[1] = p0.y;
+                a[2] = p1.x;
+                a[3] = p1.y;
+            } else {
+#pragma unroll
+                for (int t = 0; t < 4; t++) a[t] = (rin && col + t < ke) ? mrow[col + t] : 0.0;
+            }
+#pragma unroll
+            for (int s4 = 0; s4 < 4; s4++) {
+                const double* xr = xs + (g + m4 + s4) * kXs;
+                dmma884(c0a, c0b, a[s4], xr[gq]);
+                dmma884(c1a, c1b, a[s4], xr[8 + gq]);
+            }
+        }
+    }
+    if (rin) {
+        double* P = part + (size_t)blockIdx.y * kMaxRhs * ldx;
+        const int cb = 2 * (lane & 3);
+        P[(size_t)cb * ldx + row] = c0a;
+        P[(size_t)(cb + 1) * ldx + row] = c0b;
+        P[(size_t)(8 + cb) * ldx + row] = c1a;
+        P[(size_t)(9 + cb) * ldx + row] = c1b;
+    }
+}
+
+// Y[c][i] = scale_i (sum_z part[z][c][i] + shift s[c]) for i < n (scale, s optional).
+__global__ void mrhs_reduce_kernel(const double* __restrict__ part, int32_t nsplit, int32_t n,
+                                   int32_t ldx, int32_t nr, const double* __restrict__ scale,
+                                   double shift, const double* __restrict__ s,
+                                   double* __restrict__ Y) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nr * n) return;
+    const int c = (int)(t / n);
+    const int32_t i = (int32_t)(t % n);
+    double acc = 0.0;
+    for (int z = 0; z < nsplit; z++) acc += part[((size_t)z * kMaxRhs + c) * ldx + i];
+    if (s) acc += shift * s[c];
+    if (scale) acc *= scale[i];
+    Y[(size_t)c * ldx + i] = acc;
+}
+
+// FP64 copies of the inverse factor: Zd = Z on lower tiles (diagonal tiles
+// included, their upper parts are zero), Wd = W on upper tiles.
+__global__ void factor_to_f64_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
+                                     const float* __restrict__ whi, const float* __restrict__ wlo,
+                                     int32_t Vp, double* __restrict__ zd, double* __restrict__ wd) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)Vp * Vp) return;
+    const int32_t i = (int32_t)(t / Vp), j = (int32_t)(t % Vp);
+    const int ti = i / kT, tj = j / kT;
+    if (ti >= tj) zd[t] = (double)zhi[t] + (double)zlo[t];
+    if (ti <= tj) wd[t] = (double)whi[t] + (double)wlo[t];
+}
+
+// out[c] = sum_i a[c][i] b[c][i] w_i^2 (w null -> 1), one block per column.
+__global__ void col_dots_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                const double* __restrict__ w, int32_t Vp,
+                                double* __restrict__ out) {
+    __shared__ double red[8];
+    const int c = blockIdx.x;
+    double acc = 0.0;
+    for (int32_t i = threadIdx.x; i < Vp; i += blockDim.x) {
+        double t = a[(size_t)c * Vp + i] * b[(size_t)c * Vp + i];
+        if (w) t *= w[i] * w[i];
+        acc += t;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) t += red[ww];
+        out[c] = t;
+    }
+}
+
+// alpha_c = rz[c] / pq[c]; X += alpha P; R -= alpha Q
+__global__ void cg_update_xr_kernel(double* __restrict__ X, double* __restrict__ R,
+                                    const double* __restrict__ P, const double* __restrict__ Q,
+                                    const double* __restrict__ rz, const double* __restrict__ pq,
+                                    int32_t Vp, int32_t nr) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nr * Vp) return;
+    const int c = (int)(t / Vp);
+    const double al = pq[c] != 0.0 ? rz[c] / pq[c] : 0.0;
+    X[t] += al * P[t];
+    R[t] -= al * Q[t];
+}
+
+// P = Z + beta P with beta_c = rz_new[c] / rz_old[c]
+__global__ void cg_update_p_kernel(double* __restrict__ P, const double* __restrict__ Zv,
+                                   const double* __restrict__ rz_new,
+                                   const double* __restrict__ rz_old, int32_t Vp, int32_t nr) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nr * Vp) return;
+    const int c = (int)(t / Vp);
+    const double be = rz_old[c] != 0.0 ? rz_new[c] / rz_old[c] : 0.0;
+    P[t] = Zv[t] + be * P[t];
+}
+
+// R = D B (scaled right-hand sides, pad 0); X = 0
+__global__ void cg_init_kernel(const double* __restrict__ B, const double* __restrict__ d,
+                               int32_t V, int32_t Vp, int32_t nr, double* __restrict__ R,
+                               double* __restrict__ X) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nr * Vp) return;
+    const int c = (int)(t / Vp), i = (int)(t % Vp);
+    R[t] = i < V ? d[i] * B[(size_t)c * V + i] : 0.0;
+    X[t] = 0.0;
+}
+
+// B[c][i] = d_i X[c][i] for i < V (unscale)
+__global__ void cg_final_kernel(const double* __restrict__ X, const double* __restrict__ d,
+                                int32_t V, int32_t Vp, int32_t nr, double* __restrict__ B) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nr * V) return;
+    const int c = (int)(t / V), i = (int)(t % V);
+    B[t] = d[i] * X[(size_t)c * Vp + i];
+}
+
+inline unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+int32_t make_split(tpe_ctx* ctx, DevBuf& hi, DevBuf& lo, int32_t rows, int32_t cols,
+                   tc::SplitMat& m) {
+    const size_t bytes = sizeof(float) * (size_t)rows * cols;
+    TPE_TRY(ensure(ctx, hi, bytes));
+    TPE_TRY(ensure(ctx, lo, bytes));
+    if (m.hi != hi.as<float>() || m.lo != lo.as<float>() || m.rows != rows || m.cols != cols ||
+        m.ld != cols) {
+        m.hi = hi.as<float>();
+        m.lo = lo.as<float>();
+        m.rows = rows;
+        m.cols = cols;
+        m.ld = cols;
+        if (!tc::make_maps(m)) {
+            m.hi = m.lo = nullptr;
+            set_error(ctx, TPE_ERR_CUDA, "cuTensorMapEncodeTiled failed for the FP32 factor");
+            return TPE_ERR_CUDA;
+        }
+    }
+    return TPE_OK;
+}
+
+#define TC_TRY(expr) TPE_CUDA_TRY(expr)
+
+}  // namespace
+
+int32_t mixed_padded_size(int32_t V) {
+    int32_t vp = kT;
+    while (vp < V) vp *= 2;
+    return vp;
+}
+
+// FP32 factorization and inverse of the scaled A_rho (steps 1-3 above).
+// *ok = false when the FP32 factorization broke down.
+int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, bool* ok) {
+    MixedFactor& mf = ctx->mf;
+    *ok = false;
+    mf.valid = false;
+    const int32_t Vp = mixed_padded_size(V);
+    const cudaStream_t st = ctx->stream;
+    mf.V = V;
+    mf.Vp = Vp;
+    mf.rho = rho;
+    const double shift = rho / V;
+    TPE_TRY(ensure(ctx, ctx->mx_d, sizeof(double) * Vp));
+    TPE_TRY(ensure(ctx, ctx->mx_dinv, sizeof(double) * Vp));
+    TPE_TRY(ensure(ctx, ctx->mx_S, sizeof(float) * (size_t)Vp * Vp));
+    TPE_TRY(make_split(ctx, ctx->mx_Lhi, ctx->mx_Llo, Vp, Vp, mf.L));
+    TPE_TRY(make_split(ctx, ctx->mx_Zhi, ctx->mx_Zlo, Vp, Vp, mf.Z));
+    TPE_TRY(make_split(ctx, ctx->mx_Whi, ctx->mx_Wlo, Vp, Vp, mf.W));
+    if (Vp > kT) TPE_TRY(make_split(ctx, ctx->mx_Thi, ctx->mx_Tlo, Vp / 2, Vp / 2, mf.T));
+    TPE_TRY(ensure(ctx, ctx->mx_Zd, sizeof(double) * (size_t)Vp * Vp));
+    TPE_TRY(ensure(ctx, ctx->mx_Wd, sizeof(double) * (size_t)Vp * Vp));
+    TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
+    int32_t* d_bad = ctx->status.as<int32_t>() + 2;
+    TPE_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 2 * sizeof(int32_t), st));
+    int32_t* d_err = d_bad + 1;
+    double* d = ctx->mx_d.as<double>();
+    float* S = ctx->mx_S.as<float>();
+    tc::SplitMat Sm;  // the trailing matrix as a plain FP32 GEMM output
+    Sm.hi = S;
+    Sm.lo = nullptr;
+    Sm.rows = Sm.cols = Sm.ld = Vp;
+    const int nb = Vp / kT;
+    const size_t potrf_smem = sizeof(float) * (2 * kT * kLd + 96 * kPl + kT);
+    TPE_CUDA_TRY(cudaFuncSetAttribute(potrf128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)potrf_smem));
+    // Look-ahead: after panel j is solved (trsm), the main stream updates only
+    // the next block column (strip) and moves on to factor it, while the low
+    // priority stream applies panel j to the rest of the trailing matrix. The
+    // strip of step j and the rest of step j-1 write the same block column, so
+    // the strip waits for that rest.
+    while ((int32_t)ctx->fac_events.size() < 2 * nb + 2) {
+        cudaEvent_t e;
+        TPE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->fac_events.push_back(e);
+    }
+    cudaEvent_t* ev_t = ctx->fac_events.data();        // trsm of panel j done
+    cudaEvent_t* ev_r = ctx->fac_events.data() + nb;   // rest of panel j done
+    const cudaStream_t st2 = ctx->stream2;
+    {
+        const int64_t nrest = nb > 2 ? nb - 2 : 0;
+        KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + 3 * (int64_t)(nb - 1) + nrest);
+        jacobi_kernel<<<nblk(Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, ctx->mx_dinv.as<double>());
+        scale_to_f32_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, S);
+        TPE_CUDA_TRY(cudaGetLastError());
+        int last_rest = -1;
+        for (int j = 0; j < nb; j++) {
+            const int32_t j0 = j * kT;
+            potrf128_kernel<<<1, 256, potrf_smem, st>>>(S, Vp, j0, mf.L.hi, mf.L.lo, mf.Z.hi,
+                                                        mf.Z.lo, mf.W.hi, mf.W.lo, d_bad);
+            TPE_CUDA_TRY(cudaGetLastError());
+            if (j + 1 == nb) break;
+            const int32_t rows = Vp - j0 - kT;
+            split_copy_kernel<<<nblk((int64_t)rows * kT, 256), 256, 0, st>>>(
+                S, Vp, j0 + kT, j0, rows, mf.L.hi, mf.L.lo);
+            TPE_CUDA_TRY(cudaGetLastError());
+            tc::GemmArgs t;  // L21 = S21 Z_jj^T (in place in L)
+            t.a_r0 = j0 + kT;
+            t.a_c0 = j0;
+            t.b_r0 = j0;
+            t.b_c0 = j0;
+            t.c_r0 = j0 + kT;
+            t.c_c0 = j0;
+            t.M = rows;
+            t.N = kT;
+            t.K = kT;
+            TC_TRY(tc::gemm_nt(mf.L, mf.Z, mf.L, t, d_err, st));
+            if (rows > kT) {
+                // rest: S[j0+256.., j0+256..] -= L21 L21^T on lower tiles (low priority stream)
+                TPE_CUDA_TRY(cudaEventRecord(ev_t[j], st));
+                TPE_CUDA_TRY(cudaStreamWaitEvent(st2, ev_t[j], 0));
+                tc::GemmArgs u;
+                u.a_r0 = u.b_r0 = j0 + 2 * kT;
+                u.a_c0 = u.b_c0 = j0;
+                u.c_r0 = u.c_c0 = j0 + 2 * kT;
+                u.M = u.N = rows - kT;
+                u.K = kT;
+                u.mode = tc::kLowerTiles;
+                u.alpha = -1.0f;
+                u.beta = 1.0f;
+                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2));
+                TPE_CUDA_TRY(cudaEventRecord(ev_r[j], st2));
+            }
+            if (last_rest >= 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[last_rest], 0));
+            if (rows > kT) last_rest = j;
+            tc::GemmArgs v;  // strip: block column j+1 (rows j0+128..) -= L21 L21[0:128]^T
+            v.a_r0 = j0 + kT;
+            v.a_c0 = j0;
+            v.b_r0 = j0 + kT;
+            v.b_c0 = j0;
+            v.c_r0 = j0 + kT;
+            v.c_c0 = j0 + kT;
+            v.M = rows;
+            v.N = kT;
+            v.K = kT;
+            v.alpha = -1.0f;
+            v.beta = 1.0f;
+            TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, v, d_err, st));
+        }
+        if (last_rest >= 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[last_rest], 0));
+    }
+    {
+        // Z = L^{-1} level by level (W = Z^T alongside)
+        int levels = 0;
+        for (int32_t m = kT; m < Vp; m *= 2) levels++;
+        KernelScope ks(ctx, TPE_KGROUP_TRSV, 3 * (int64_t)levels);
+        for (int32_t m = kT; m < Vp; m *= 2) {
+            const int32_t npairs = Vp / (2 * m);
+            tc::GemmArgs t;  // T^T = W11 L21^T
+            t.a_zr = t.a_zc = 2 * m;
+            t.b_r0 = m;
+            t.b_zr = t.b_zc = 2 * m;
+            t.c_zr = m;
+            t.M = t.N = t.K = m;
+            t.mode = tc::kAUpper;
+            t.nbatch = npairs;
+            TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T, t, d_err, st));
+            tc::GemmArgs u;  // Z21 = -Z22 T
+            u.a_r0 = u.a_c0 = m;
+            u.a_zr = u.a_zc = 2 * m;
+            u.b_zr = m;
+            u.c_r0 = m;
+            u.c_zr = u.c_zc = 2 * m;
+            u.M = u.N = u.K = m;
+            u.mode = tc::kALower;
+            u.alpha = -1.0f;
+            u.nbatch = npairs;
+            TC_TRY(tc::gemm_nt(mf.Z, mf.T, mf.Z, u, d_err, st));
+            transpose_block_kernel<<<dim3(m / 32, m / 32, npairs), dim3(32, 8), 0, st>>>(
+                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, m);
+            TPE_CUDA_TRY(cudaGetLastError());
+        }
+    }
+    {
+        KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
+        factor_to_f64_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(
+            mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, ctx->mx_Zd.as<double>(), ctx->mx_Wd.as<double>());
+        TPE_CUDA_TRY(cudaGetLastError());
+    }
+    int32_t flags[2] = {0, 0};
+    TPE_CUDA_TRY(cudaMemcpyAsync(flags, d_bad, sizeof(flags), cudaMemcpyDeviceToHost, st));
+    TPE_CUDA_TRY(cudaStreamSynchronize(st));
+    if (flags[1]) {
+        set_error(ctx, TPE_ERR_DEVICE_TIMEOUT, "tensor-core pipeline wait timed out");
+        return TPE_ERR_DEVICE_TIMEOUT;
+    }
+    *ok = flags[0] == 0;
+    mf.valid = *ok;
+    return TPE_OK;
+}
+
+// Solves A_rho X = B for nr right-hand sides (B, X: [nr][V] FP64 device; may
+// alias) by CG on the scaled system preconditioned with the FP32 inverse factor.
+// *iters = iterations of the last pass; *converged = every column reached
+// ||B - A_rho X|| <= tol ||B||.
+int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* d_X, int32_t nr,
+                    int32_t maxit, double tol, int32_t* iters, bool* converged) {
+    const MixedFactor& mf = ctx->mf;
+    const int32_t V = mf.V, Vp = mf.Vp;
+    const double shift = mf.rho / V;
+    const cudaStream_t st = ctx->stream;
+    *converged = true;
+    *iters = 0;
+    const size_t vec = (size_t)kMaxRhs * Vp;
+    TPE_TRY(ensure(ctx, ctx->mx_vec, sizeof(double) * (6 * vec + 8 * kMaxRhs)));
+    constexpr int kSplit = 8;
+    TPE_TRY(ensure(ctx, ctx->mx_part, sizeof(double) * (size_t)kSplit * kMaxRhs * Vp));
+    double* X = ctx->mx_vec.as<double>();
+    double* R = X + vec;
+    double* P = R + vec;
+    double* Q = P + vec;
+    double* Zv = Q + vec;
+    double* U = Zv + vec;
+    double* sc = U + vec;  // 8 arrays of kMaxRhs scalars
+    double* s_sum = sc;
+    double* pq = sc + kMaxRhs;
+    double* rz[2] = {sc + 2 * kMaxRhs, sc + 3 * kMaxRhs};
+    double* res2 = sc + 4 * kMaxRhs;
+    double* bn2 = sc + 5 * kMaxRhs;
+    double* part = ctx->mx_part.as<double>();
+    const double* d = ctx->mx_d.as<double>();
+    const double* Zd = ctx->mx_Zd.as<double>();
+    const double* Wd = ctx->mx_Wd.as<double>();
+    std::vector<double> hres(kMaxRhs), hbn(kMaxRhs);
+    int32_t max_iters = 0;
+    const unsigned rb_V = (unsigned)((V + kMvRows - 1) / kMvRows);
+    const unsigned rb_Vp = (unsigned)(Vp / kMvRows);
+    for (int32_t c0 = 0; c0 < nr; c0 += kMaxRhs) {
+        const int32_t n = nr - c0 < kMaxRhs ? nr - c0 : kMaxRhs;
+        const int64_t tot = (int64_t)n * Vp;
+        // out = W (Z in): the preconditioner (L L^T)^{-1} of the scaled system
+        auto precond = [&](const double* in, double* out) -> int32_t {
+            KernelScope ks(ctx, TPE_KGROUP_TRSV, 4);
+            mrhs_dmma_kernel<1><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Zd, Vp, Vp, in, Vp, n, part);
+            mrhs_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, kSplit, Vp, Vp, n, nullptr, 0.0,
+                                                                nullptr, U);
+            mrhs_dmma_kernel<2><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Wd, Vp, Vp, U, Vp, n, part);
+            mrhs_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, kSplit, Vp, Vp, n, nullptr, 0.0,
+                                                                nullptr, out);
+            TPE_CUDA_TRY(cudaGetLastError());
+            return TPE_OK;
+        };
+        // out = S in = D (A + shift 1 1^T) D in, rows < V
+        auto matvec = [&](const double* in, double* out) -> int32_t {
+            KernelScope ks(ctx, TPE_KGROUP_OTHER, 3);
+            cg_prep_kernel<<<n, 256, 0, st>>>(in, d, V, Vp, U, s_sum);
+            mrhs_dmma_kernel<0><<<dim3(rb_V, kSplit), 256, 0, st>>>(d_A, V, V, U, Vp, n, part);
+            mrhs_reduce_kernel<<<nblk((int64_t)n * V, 256), 256, 0, st>>>(part, kSplit, V, Vp, n, d,
+                                                                           shift, s_sum, out);
+            TPE_CUDA_TRY(cudaGetLastError());
+            return TPE_OK;
+        };
+        auto dots = [&](const double* a, const double* b, const double* w, double* out) -> int32_t {
+            KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+            col_dots_kernel<<<n, 256, 0, st>>>(a, b, w, Vp, out);
+            TPE_CUDA_TRY(cudaGetLastError());
+            return TPE_OK;
+        };
+        {
+            KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+            cg_init_kernel<<<nblk(tot, 256), 256, 0, st>>>(d_B + (size_t)c0 * V, d, V, Vp, n, R, X);
+            TPE_CUDA_TRY(cudaGetLastError());
+        }
+        // the matrix-vector kernel writes rows < V only: the pad of Q stays 0
+        TPE_CUDA_TRY(cudaMemsetAsync(Q, 0, sizeof(double) * tot, st));
+        // residual norms of the unscaled system: ||D^{-1} R||
+        const double* di = ctx->mx_dinv.as<double>();
+        TPE_TRY(dots(R, R, di, bn2));
+        TPE_CUDA_TRY(cudaMemcpyAsync(hbn.data(), bn2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        TPE_TRY(precond(R, Zv));
+        TPE_CUDA_TRY(cudaMemcpyAsync(P, Zv, sizeof(double) * tot, cudaMemcpyDeviceToDevice, st));
+        TPE_TRY(dots(R, Zv, nullptr, rz[0]));
+        int it = 0;
+        bool done = false;
+        for (it = 1; it <= maxit; it++) {
+            TPE_TRY(matvec(P, Q));
+            TPE_TRY(dots(P, Q, nullptr, pq));
+            {
+                KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+                cg_update_xr_kernel<<<nblk(tot, 256), 256, 0, st>>>(X, R, P, Q, rz[(it - 1) & 1], pq, Vp, n);
+                TPE_CUDA_TRY(cudaGetLastError());
+            }
+            TPE_TRY(dots(R, R, di, res2));
+            TPE_CUDA_TRY(cudaMemcpyAsync(hres.data(), res2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+            TPE_CUDA_TRY(cudaStreamSynchronize(st));
+            done = true;
+            for (int c = 0; c < n; c++)
+                if (!(hres[c] <= tol * tol * hbn[c])) done = false;
+            if (done) break;
+            TPE_TRY(precond(R, Zv));
+            TPE_TRY(dots(R, Zv, nullptr, rz[it & 1]));
+            {
+                KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+                cg_update_p_kernel<<<nblk(tot, 256), 256, 0, st>>>(P, Zv, rz[it & 1], rz[(it - 1) & 1], Vp, n);
+                TPE_CUDA_TRY(cudaGetLastError());
+            }
+        }
+        if (!done) *converged = false;
+        if (it > max_iters) max_iters = it > maxit ? maxit : it;
+        {
+            KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+            cg_final_kernel<<<nblk((int64_t)n * V, 256), 256, 0, st>>>(X, d, V, Vp, n, d_X + (size_t)c0 * V);
+            TPE_CUDA_TRY(cudaGetLastError());
+        }
+    }
+    *iters = max_iters;
+    return TPE_OK;
+}
+
+}  // namespace tpe

@@ -1,0 +1,414 @@
+// 3xTF32 tensor-core GEMM for sm_100a: C = alpha * A * B^T + beta * C on
+// split-FP32 matrices (tc.h).
+//
+// One CTA computes one 128 x 128 output tile with the fifth-generation tensor
+// cores: operand tiles arrive by TMA (128B swizzle, K-major) into a 3-stage
+// shared-memory ring, one elected thread issues tcgen05.mma (kind::tf32,
+// M=128, N=128, K=8) with the FP32 accumulator in tensor memory, and the four
+// warps read the accumulator back with tcgen05.ld for the epilogue, which
+// adds beta * C and writes C again as a split pair. Every wait on a pipeline
+// barrier is bounded: when one gives up, the kernel raises *err, lets the
+// copies it issued land, frees its tensor memory and returns.
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "tc.h"
+
+namespace tpe {
+namespace tc {
+namespace {
+
+constexpr int kStages = 3;
+constexpr int kTileBytes = kBM * kBK * 4;  // one 128 x 32 FP32 operand tile (A and B alike)
+constexpr int kStageBytes = 4 * kTileBytes;  // A_hi, A_lo, B_hi, B_lo
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 128;
+constexpr int kTmemCols = 128;
+// Instruction descriptor of tcgen05.mma kind::tf32: D format F32 (bits 4-5),
+// A and B format TF32 (bits 7-9, 10-12), both K-major, N >> 3 at bit 17,
+// M >> 4 at bit 24.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) |
+                            ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+constexpr long long kWaitCycles = 4000000000LL;  // about 2 s at 1.9 GHz
+
+struct KParams {
+    GemmArgs g;
+    float* c_hi;
+    float* c_lo;
+    int32_t ldc;
+    int32_t* err;
+};
+
+__host__ __device__ __forceinline__ void split(float x, float& hi, float& lo) {
+    // round to nearest (ties away) at TF32 precision, then the exact remainder
+    union {
+        float f;
+        uint32_t u;
+    } v;
+    v.f = x;
+    v.u = (v.u + 0x1000u) & 0xFFFFE000u;
+    hi = v.f;
+    lo = x - hi;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of parity `parity` to complete; false (and *err = 1)
+// when it has not completed within kWaitCycles.
+__device__ bool mbar_wait(uint32_t a, uint32_t parity, int32_t* err) {
+    if (mbar_try(a, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try(a, parity)) {
+        if (clock64() - t0 > kWaitCycles) {
+            if (err) atomicExch(err, 1);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t mbar,
+                                            int32_t x, int32_t y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(mbar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major operand, 128B swizzle, 8-row groups
+// 1024 bytes apart (SBO), descriptor version 1 (bit 46), layout 2 = SWIZZLE_128B.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) |
+           ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     mbar)
+                 : "memory");
+}
+
+// 32 consecutive accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(128, 1)
+gemm_nt_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__ CUtensorMap a_lo,
+               const __grid_constant__ CUtensorMap b_hi, const __grid_constant__ CUtensorMap b_lo,
+               const KParams P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(smem + kStages * kStageBytes);  // full[S], empty[S], done
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * kStages + 1);
+    volatile int32_t* aborted = (volatile int32_t*)(tmem_slot + 1);
+    const GemmArgs& g = P.g;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int z = blockIdx.z;
+
+    int ti, tj;
+    if (g.mode & kLowerTiles) {
+        const int x = blockIdx.x;
+        int t = (int)((sqrtf(8.0f * (float)x + 1.0f) - 1.0f) * 0.5f);
+        while ((t + 1) * (t + 2) / 2 <= x) t++;
+        while (t * (t + 1) / 2 > x) t--;
+        ti = t;
+        tj = x - t * (t + 1) / 2;
+    } else {
+        ti = blockIdx.y;
+        tj = blockIdx.x;
+    }
+    int k_begin = 0, k_end = g.K;
+    if (g.mode & kAUpper) k_begin = min(g.K, ti * kBM);
+    if (g.mode & kALower) k_end = min(g.K, (ti + 1) * kBM);
+    const int nk = k_end > k_begin ? (k_end - k_begin) / kBK : 0;
+
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages),
+                   done = smem_u32(bars + 2 * kStages);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(done, 1);
+        *aborted = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    const int32_t ax = g.a_c0 + z * g.a_zc + k_begin, ay = g.a_r0 + z * g.a_zr + ti * kBM;
+    const int32_t bx = g.b_c0 + z * g.b_zc + k_begin, by = g.b_r0 + z * g.b_zr + tj * kBN;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        int issued = 0;
+        for (int it = 0; it < nk; it++) {
+            const int s = it % kStages;
+            if (it >= kStages && !mbar_wait(empty0 + 8 * s, ((it / kStages) - 1) & 1, P.err)) {
+                *aborted = 1;
+                break;
+            }
+            if (*aborted) break;
+            const uint32_t st = smem_u32(smem + s * kStageBytes);
+            const uint32_t fb = full0 + 8 * s;
+            mbar_expect_tx(fb, kStageBytes);
+            const int32_t k = it * kBK;
+            tma_load_2d(st, &a_hi, fb, ax + k, ay);
+            tma_load_2d(st + kTileBytes, &a_lo, fb, ax + k, ay);
+            tma_load_2d(st + 2 * kTileBytes, &b_hi, fb, bx + k, by);
+            tma_load_2d(st + 3 * kTileBytes, &b_lo, fb, bx + k, by);
+            issued = it + 1;
+        }
+        // every copy issued has landed before the CTA may exit
+        for (int it = issued > kStages ? issued - kStages : 0; it < issued; it++)
+            mbar_wait(full0 + 8 * (it % kStages), (it / kStages) & 1, P.err);
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer: D += Ahi*Bhi + Ahi*Blo + Alo*Bhi per K=8 step
+        for (int it = 0; it < nk; it++) {
+            const int s = it % kStages;
+            if (!mbar_wait(full0 + 8 * s, (it / kStages) & 1, P.err)) {
+                *aborted = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = smem_u32(smem + s * kStageBytes);
+#pragma unroll
+            for (int kk = 0; kk < kBK / 8; kk++) {
+                const uint64_t ah = sw128_desc(st + kk * 32);
+                const uint64_t al = sw128_desc(st + kTileBytes + kk * 32);
+                const uint64_t bh = sw128_desc(st + 2 * kTileBytes + kk * 32);
+                const uint64_t bl = sw128_desc(st + 3 * kTileBytes + kk * 32);
+                mma_tf32(tmem, ah, bh, (it | kk) ? 1u : 0u);
+                mma_tf32(tmem, ah, bl, 1u);
+                mma_tf32(tmem, al, bh, 1u);
+            }
+            mma_commit(empty0 + 8 * s);
+        }
+        if (nk > 0)
+            mma_commit(done);
+        else
+            mbar_arrive(done);
+    }
+    __syncwarp();
+    __syncthreads();
+
+    bool ok = mbar_wait(done, 0, P.err);
+    ok = __all_sync(0xffffffffu, ok) && !*aborted;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+        const int row = ti * kBM + warp * 32 + lane;
+        const bool rin = row < g.M;
+        const int32_t cr = g.c_r0 + z * g.c_zr + (rin ? row : 0);
+        const int32_t cc = g.c_c0 + z * g.c_zc;
+        float* ch = P.c_hi + (size_t)cr * P.ldc + cc;
+        float* cl = P.c_lo ? P.c_lo + (size_t)cr * P.ldc + cc : nullptr;
+        const bool vec_ok = (cc & 3) == 0;
+        const float alpha = g.alpha, beta = g.beta;
+        for (int c0 = 0; c0 < kBN; c0 += 32) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (!rin) continue;
+            const int col0 = tj * kBN + c0;
+            if (!cl) {
+                // plain FP32 output
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int col = col0 + 4 * q;
+                    if (vec_ok && col + 3 < g.N) {
+                        float4 y = make_float4(alpha * v[4 * q], alpha * v[4 * q + 1],
+                                               alpha * v[4 * q + 2], alpha * v[4 * q + 3]);
+                        if (beta != 0.0f) {
+                            const float4 h = *reinterpret_cast<const float4*>(ch + col);
+                            y.x += beta * h.x;
+                            y.y += beta * h.y;
+                            y.z += beta * h.z;
+                            y.w += beta * h.w;
+                        }
+                        *reinterpret_cast<float4*>(ch + col) = y;
+                    } else {
+                        for (int e = 0; e < 4; e++) {
+                            if (col + e >= g.N) break;
+                            float y = alpha * v[4 * q + e];
+                            if (beta != 0.0f) y += beta * ch[col + e];
+                            ch[col + e] = y;
+                        }
+                    }
+                }
+                continue;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int col = col0 + 4 * q;
+                if (vec_ok && col + 3 < g.N) {
+                    float y[4] = {alpha * v[4 * q], alpha * v[4 * q + 1], alpha * v[4 * q + 2],
+                                  alpha * v[4 * q + 3]};
+                    if (beta != 0.0f) {
+                        const float4 h = *reinterpret_cast<const float4*>(ch + col);
+                        const float4 l = *reinterpret_cast<const float4*>(cl + col);
+                        y[0] += beta * (h.x + l.x);
+                        y[1] += beta * (h.y + l.y);
+                        y[2] += beta * (h.z + l.z);
+                        y[3] += beta * (h.w + l.w);
+                    }
+                    float4 h, l;
+                    split(y[0], h.x, l.x);
+                    split(y[1], h.y, l.y);
+                    split(y[2], h.z, l.z);
+                    split(y[3], h.w, l.w);
+                    *reinterpret_cast<float4*>(ch + col) = h;
+                    *reinterpret_cast<float4*>(cl + col) = l;
+                } else {
+                    for (int e = 0; e < 4; e++) {
+                        if (col + e >= g.N) break;
+                        float y = alpha * v[4 * q + e];
+                        if (beta != 0.0f) y += beta * (ch[col + e] + cl[col + e]);
+                        float h, l;
+                        split(y, h, l);
+                        ch[col + e] = h;
+                        cl[col + e] = l;
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols)
+                     : "memory");
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+bool encode(CUtensorMap* map, float* base, int32_t rows, int32_t cols, int32_t ld) {
+    auto enc = encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBM};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool make_maps(SplitMat& m) {
+    if (!m.hi || !m.lo || m.rows <= 0 || m.cols <= 0 || m.ld % 32 != 0 || m.cols > m.ld) return false;
+    if (((uintptr_t)m.hi | (uintptr_t)m.lo) & 127) return false;
+    return encode(&m.map_hi, m.hi, m.rows, m.cols, m.ld) &&
+           encode(&m.map_lo, m.lo, m.rows, m.cols, m.ld);
+}
+
+cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const GemmArgs& g,
+                    int32_t* err, cudaStream_t stream) {
+    if (g.M <= 0 || g.N <= 0 || g.nbatch <= 0) return cudaSuccess;
+    // TMA x coordinates must be multiples of 4 FP32 elements (16 bytes); whole
+    // K stages only (callers pad to 128).
+    if (g.K < 0 || g.K % kBK != 0 || ((g.a_c0 | g.a_zc | g.b_c0 | g.b_zc) & 3) != 0 ||
+        g.a_c0 < 0 || g.a_r0 < 0 || g.b_c0 < 0 || g.b_r0 < 0 || g.a_zc < 0 || g.a_zr < 0 ||
+        g.b_zc < 0 || g.b_zr < 0 || !C.hi)
+        return cudaErrorInvalidValue;
+    // every element the epilogue writes lies inside C
+    const int64_t last_r = (int64_t)g.c_r0 + (int64_t)(g.nbatch - 1) * g.c_zr + g.M;
+    const int64_t last_c = (int64_t)g.c_c0 + (int64_t)(g.nbatch - 1) * g.c_zc + g.N;
+    if (g.c_r0 < 0 || g.c_c0 < 0 || g.c_zr < 0 || g.c_zc < 0 || last_r > C.rows || last_c > C.cols)
+        return cudaErrorInvalidValue;
+    const int tm = (g.M + kBM - 1) / kBM, tn = (g.N + kBN - 1) / kBN;
+    dim3 grid;
+    if (g.mode & kLowerTiles) {
+        if (tm != tn) return cudaErrorInvalidValue;
+        grid = dim3((unsigned)(tm * (tm + 1) / 2), 1, (unsigned)g.nbatch);
+    } else {
+        grid = dim3((unsigned)tn, (unsigned)tm, (unsigned)g.nbatch);
+    }
+    cudaError_t e = cudaFuncSetAttribute(gemm_nt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kSmemBytes);
+    if (e != cudaSuccess) return e;
+    KParams P;
+    P.g = g;
+    P.c_hi = C.hi;
+    P.c_lo = C.lo;
+    P.ldc = C.ld;
+    P.err = err;
+    gemm_nt_kernel<<<grid, 128, kSmemBytes, stream>>>(A.map_hi, A.map_lo, B.map_hi, B.map_lo, P);
+    return cudaGetLastError();
+}
+
+}  // namespace tc
+}  // namespace tpe

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/tpe.h"
+#include "tc.h"
 
 #define TPE_CUDA_TRY(expr)                                                              \
     do {                                                                                \
@@ -38,6 +39,9 @@ struct DevBuf {
 
 // Dense Cholesky block size (diagonal blocks are factored by one CTA).
 constexpr int kNB = 64;
+// Most right-hand sides (3 per constraint row, +3 for b) the mixed solve takes
+// at factor time; larger sets use the FP64 factorization.
+constexpr int kMixedMaxRhs = 48;
 
 // Everything the structured saddle solve keeps between the factorization and
 // later solves: the frozen operator of optimizer.ts's 'frozen' projection.
@@ -45,6 +49,11 @@ struct SaddleOp {
     bool valid = false;
     int V = 0, k = 0;
     bool trans_constrained = false;  // set contains a barycenter or point block
+    bool mixed = false;              // solves use the FP32 factor + FP64 CG (mixed.cu)
+    bool mixed_fallback = false;     // mixed requested, FP64 factorization used instead
+    int refine_iters = 0;            // CG iterations of the factor-time solve
+    int refine_max_iter = 30;
+    double refine_tol = 1e-12;
     double rho = 0.0;                // A_rho = A + (rho/V) 1 1^T
     // device (views into ctx buffers)
     double* A = nullptr;     // V x V original A (unfactored, for residuals)
@@ -58,6 +67,15 @@ struct SaddleOp {
     std::vector<double> Scc;   // k x k, then its Cholesky factor (lower)
     std::vector<double> Scu;   // k x 3 = C U / rho
     std::vector<double> M;     // 3 x 3 = Scu^T Scc^{-1} Scu, then its Cholesky factor
+};
+
+// FP32 tensor-core factor of the Jacobi-scaled A_rho (mixed.cu): S ~ L L^T,
+// Z = L^{-1}, W = Z^T, all Vp x Vp split-FP32; T is the TRTRI scratch.
+struct MixedFactor {
+    bool valid = false;
+    int V = 0, Vp = 0;
+    double rho = 0.0;
+    tc::SplitMat L, Z, W, T;
 };
 
 struct DevBlock {
@@ -98,6 +116,10 @@ struct tpe_ctx {
     tpe::DevBuf rhs, sol, tmp, solve_scratch;
     tpe::DevBuf status;                     // device-side int flags
     tpe::SaddleOp op;
+    // mixed-precision factor (mixed.cu)
+    tpe::DevBuf mx_d, mx_dinv, mx_S, mx_Lhi, mx_Llo, mx_Zhi, mx_Zlo, mx_Whi, mx_Wlo, mx_Thi, mx_Tlo,
+        mx_vec, mx_part, mx_Zd, mx_Wd;
+    tpe::MixedFactor mf;
     std::vector<double> h_tmp;
 
     // instrumentation: kernel launch count and per-group CUDA-event timing
@@ -173,6 +195,16 @@ int32_t gram_dots(tpe_ctx* ctx, const double* X, int32_t nx, const double* Y, in
 // A_rho = A + shift (every entry) into L (lower triangle copied), and trace(A) into *d_trace.
 int32_t shift_copy(tpe_ctx* ctx, const double* d_A, double* d_L, int32_t n, double shift);
 int32_t trace(tpe_ctx* ctx, const double* d_A, int32_t n, double* d_out);
+
+// ---- mixed-precision solve (mixed.cu) ------------------------------------
+int32_t mixed_padded_size(int32_t V);
+// FP32 tensor-core factor + inverse of the Jacobi-scaled A_rho = A + (rho/V) 1 1^T
+// into ctx->mf; *ok = false when the FP32 factorization broke down.
+int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, bool* ok);
+// A_rho X = B for nr right-hand sides ([nr][V], FP64, may alias) by CG with the
+// FP32 factor as preconditioner, to ||B - A_rho X|| <= tol ||B|| per column.
+int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* d_X, int32_t nr,
+                    int32_t maxit, double tol, int32_t* iters, bool* converged);
 
 // ---- constraints (constraints.cu) -----------------------------------------
 // Upload the set, returns k (stacked rows).
