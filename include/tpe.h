@@ -104,7 +104,9 @@ typedef struct {
     double proj_tol_abs, proj_tol_rel;         /* 1e-4, 1e-4 */
     int32_t proj_max_iter;                     /* 8 */
     int32_t precision;             /* TPE_PRECISION_* (extension) */
-    int32_t trials;                /* tau trials evaluated per batched launch (extension; 1 = sequential) */
+    int32_t trials;                /* frozen projection: step sizes projected together per batch
+                                      (extension; default 8, 1 = one at a time; the accepted tau
+                                      and vertices do not depend on it) */
     int32_t collect_field;         /* write g~ into descent_field when non-null */
     int32_t refine_max_iter;       /* mixed path: FP64 refinement cap (extension) */
     int32_t reserved;

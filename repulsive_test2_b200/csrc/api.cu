@@ -249,6 +249,37 @@ __global__ void add_flat_kernel(double* __restrict__ v3, const double* __restric
     v3[3 * i + 2] = v3[3 * i + 2] + f[2 * V + i];
 }
 
+// raw[a] = p - tau[a] dir for the trials of one batch.
+__global__ void step_batch_kernel(const double* __restrict__ p, const double* __restrict__ dir,
+                                  const double* __restrict__ taus, int64_t n,
+                                  double* __restrict__ out) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[(int64_t)blockIdx.y * n + t] = p[t] - taus[blockIdx.y] * dir[t];
+}
+
+// One projection correction for each active trial a = idx[y]: the Newton step
+// x = -sum_s Y[s] lam_a[s] - mu_a[c] / (rho sqrt V) (the same operations, in the
+// same order, as combine_kernel) added to the positions cur[a]; bad[a] = 1 when
+// x has a non-finite entry (the trial is then abandoned).
+__global__ void proj_update_kernel(double* __restrict__ cur, int64_t stride,
+                                   const double* __restrict__ Y, int32_t k,
+                                   const double* __restrict__ coef, const int32_t* __restrict__ idx,
+                                   int32_t V, int32_t* __restrict__ bad) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t m = 3 * (int64_t)V;
+    if (t >= m) return;
+    const int a = idx[blockIdx.y];
+    const double* cf = coef + (size_t)blockIdx.y * (k + 3);
+    double v = 0.0;
+    for (int32_t s2 = 0; s2 < k; s2++) v -= Y[(int64_t)s2 * m + t] * cf[s2];
+    const int c = (int)(t / V);
+    v -= cf[k + c];
+    if (!isfinite(v)) bad[a] = 1;
+    const int64_t i = t % V;
+    double* q = cur + (int64_t)a * stride + 3 * i + c;
+    *q = *q + v;
+}
+
 __global__ void step_kernel(const double* __restrict__ p, const double* __restrict__ dir,
                             double tau, int64_t n, double* __restrict__ out) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -476,6 +507,35 @@ int32_t op_build(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k, 
     return op_finalize(ctx, V, k, singular, b_flat, o);
 }
 
+// Multipliers of the bordered Schur system for the reduced right-hand side
+// rc = C w - d (k) and ru = U^T w (3): lam (k) and mu (3).
+void schur_multipliers(const SaddleOp& op, const std::vector<double>& rc, const double* ru,
+                       std::vector<double>& lam, double mu[3]) {
+    const int32_t k = op.k;
+    lam.assign((size_t)k, 0.0);
+    mu[0] = mu[1] = mu[2] = 0.0;
+    if (k == 0) return;
+    std::vector<double> t = rc;
+    host_chol_solve(op.Scc, k, t);
+    if (op.trans_constrained) {
+        std::vector<double> rhs(3);
+        for (int c = 0; c < 3; c++) {
+            double s = 0;
+            for (int32_t r = 0; r < k; r++) s += op.Scu[(size_t)r * 3 + c] * t[r];
+            rhs[c] = s - ru[c];
+        }
+        host_chol_solve(op.M, 3, rhs);
+        for (int c = 0; c < 3; c++) mu[c] = rhs[c];
+        std::vector<double> r2 = rc;
+        for (int32_t r = 0; r < k; r++)
+            for (int c = 0; c < 3; c++) r2[r] -= op.Scu[(size_t)r * 3 + c] * mu[c];
+        host_chol_solve(op.Scc, k, r2);
+        lam = r2;
+    } else {
+        lam = t;
+    }
+}
+
 // Solve with the current operator: b_flat (device, 3V, or null = 0), d (host, k,
 // or null = 0). x_flat (device) and lam (host) out. residual computed when non-null.
 int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_flat,
@@ -522,29 +582,8 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
     }
     if (d)
         for (int32_t r = 0; r < k; r++) rc[r] -= d[r];
-    lam.assign((size_t)k, 0.0);
     double mu[3] = {0, 0, 0};
-    if (k > 0) {
-        std::vector<double> t = rc;
-        host_chol_solve(op.Scc, k, t);
-        if (op.trans_constrained) {
-            std::vector<double> rhs(3);
-            for (int c = 0; c < 3; c++) {
-                double s = 0;
-                for (int32_t r = 0; r < k; r++) s += op.Scu[(size_t)r * 3 + c] * t[r];
-                rhs[c] = s - ru[c];
-            }
-            host_chol_solve(op.M, 3, rhs);
-            for (int c = 0; c < 3; c++) mu[c] = rhs[c];
-            std::vector<double> r2 = rc;
-            for (int32_t r = 0; r < k; r++)
-                for (int c = 0; c < 3; c++) r2[r] -= op.Scu[(size_t)r * 3 + c] * mu[c];
-            host_chol_solve(op.Scc, k, r2);
-            lam = r2;
-        } else {
-            lam = t;
-        }
-    }
+    schur_multipliers(op, rc, ru.data(), lam, mu);
     TPE_TRY(combine_solution(ctx, b_flat ? w : nullptr, op.Y, k, lam.data(), mu, op.rho, V,
                              x_flat));
     if (residual) {
@@ -704,6 +743,116 @@ int32_t project_dev(tpe_ctx* ctx, const double* d_start, const SetInfo& S, const
     return TPE_OK;
 }
 
+// projectOntoConstraintSet (lineSearch.ts:196-295) in frozen mode for several
+// start points at once: trial a starts at start[a] (ntrial x 3V) and ends in
+// cur[a]. Each iteration evaluates Phi for every trial still running in one
+// launch and applies all their Newton corrections in one launch; the per-trial
+// decisions (converged, iteration cap, non-finite Phi, non-finite correction)
+// and their order are those of project_dev.
+int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, const SetInfo& S,
+                          const tpe_step_opts* o, double* d_cur, int32_t* ok, int32_t* iters,
+                          double* phi_norm, double* timings) {
+    const int32_t V = ctx->V, k = S.k, nb = S.nblocks;
+    const int64_t m = 3 * (int64_t)V;
+    const SaddleOp& op = ctx->op;
+    TPE_CUDA_TRY(cudaMemcpyAsync(d_cur, d_start, sizeof(double) * m * ntrial,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+    std::vector<int32_t> active;
+    for (int32_t a = 0; a < ntrial; a++) {
+        active.push_back(a);
+        ok[a] = 0;
+        iters[a] = o->proj_max_iter;
+        phi_norm[a] = INFINITY;
+    }
+    TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * (4 + 2 * (size_t)ntrial)));
+    int32_t* d_bad = ctx->status.as<int32_t>() + 4;
+    int32_t* d_idx = d_bad + ntrial;
+    TPE_CUDA_TRY(cudaMemsetAsync(d_bad, 0, sizeof(int32_t) * ntrial, ctx->stream));
+    TPE_TRY(ensure(ctx, ctx->con_red, sizeof(double) * (size_t)ntrial * ((size_t)k + 2 * nb + k + 3)));
+    double* d_phi = ctx->con_red.as<double>();
+    double* d_ns = d_phi + (size_t)ntrial * k;
+    double* d_coef = d_ns + (size_t)ntrial * 2 * nb;
+    std::vector<double> phi((size_t)ntrial * k), ns((size_t)ntrial * 2 * nb);
+    std::vector<int32_t> hbad(ntrial, 0);
+    std::vector<double> coef, lam;
+    std::vector<int32_t> upd;
+    const double ru[3] = {0.0, 0.0, 0.0};
+    for (int32_t it = 0; it <= o->proj_max_iter && !active.empty(); it++) {
+        const int32_t na = (int32_t)active.size();
+        TPE_CUDA_TRY(cudaMemcpyAsync(d_idx, active.data(), sizeof(int32_t) * na,
+                                     cudaMemcpyHostToDevice, ctx->stream));
+        TPE_TRY(eval_constraints_batch(ctx, d_cur, m, d_idx, na, nb, k, d_phi, d_ns));
+        if (k > 0)
+            TPE_CUDA_TRY(cudaMemcpyAsync(phi.data(), d_phi, sizeof(double) * na * k,
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+        TPE_CUDA_TRY(cudaMemcpyAsync(ns.data(), d_ns, sizeof(double) * na * 2 * nb,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+        TPE_CUDA_TRY(cudaMemcpyAsync(hbad.data(), d_bad, sizeof(int32_t) * ntrial,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+        TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        std::vector<int32_t> next;
+        upd.clear();
+        coef.clear();
+        for (int32_t q = 0; q < na; q++) {
+            const int32_t a = active[q];
+            if (it > 0 && hbad[a]) {  // last correction was not finite
+                iters[a] = it - 1;
+                continue;
+            }
+            const double* ph = phi.data() + (size_t)q * k;
+            const double* nsq = ns.data() + (size_t)q * 2 * nb;
+            double sq = 0.0;
+            for (int32_t r = 0; r < k; r++) sq += ph[r] * ph[r];
+            phi_norm[a] = sqrt(sq);
+            bool converged = true;
+            for (int32_t b = 0; b < nb; b++) {
+                const double bn = sqrt(nsq[2 * b]);
+                const double tol = js_max(o->proj_tol_abs, o->proj_tol_rel * nsq[2 * b + 1]);
+                if (bn > tol) {
+                    converged = false;
+                    break;
+                }
+            }
+            if (converged) {
+                ok[a] = 1;
+                iters[a] = it;
+                continue;
+            }
+            if (it == o->proj_max_iter) continue;
+            if (!all_finite(ph, (size_t)k)) {
+                iters[a] = it;
+                continue;
+            }
+            std::vector<double> rc((size_t)k);
+            for (int32_t r = 0; r < k; r++) rc[r] = 0.0 - (-ph[r]);
+            double mu[3];
+            schur_multipliers(op, rc, ru, lam, mu);
+            const double su = 1.0 / (op.rho * sqrt((double)V));
+            for (int32_t r = 0; r < k; r++) coef.push_back(lam[r]);
+            for (int c = 0; c < 3; c++) coef.push_back(mu[c] * su);
+            upd.push_back(a);
+            next.push_back(a);
+        }
+        active = next;
+        if (upd.empty()) break;
+        {
+            Timer t(ctx, timings, TPE_PHASE_SADDLE);
+            const int32_t nu = (int32_t)upd.size();
+            TPE_CUDA_TRY(cudaMemcpyAsync(d_idx, upd.data(), sizeof(int32_t) * nu,
+                                         cudaMemcpyHostToDevice, ctx->stream));
+            TPE_CUDA_TRY(cudaMemcpyAsync(d_coef, coef.data(), sizeof(double) * coef.size(),
+                                         cudaMemcpyHostToDevice, ctx->stream));
+            KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+            proj_update_kernel<<<dim3((unsigned)((m + 255) / 256), (unsigned)nu), 256, 0,
+                                 ctx->stream>>>(d_cur, m, op.Y, k, d_coef, d_idx, V, d_bad);
+            TPE_CUDA_TRY(cudaGetLastError());
+            // the host vectors must outlive the copies
+            TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        }
+    }
+    return TPE_OK;
+}
+
 void stats_reset(tpe_step_stats* st) {
     memset(st, 0, sizeof(*st));
     st->slope = NAN;
@@ -761,6 +910,65 @@ int32_t line_search_dev(tpe_ctx* ctx, const double* d_pos, const double* d_dE, c
     double tau = o->tau0;
     int32_t lastReason = TPE_REASON_TAU_BELOW_MIN;
     int32_t trials = 0;
+    if (frozen && o->trials > 1) {
+        // Batched trials: the projections of up to o->trials step sizes run
+        // together; the energies are then evaluated in the sequential order
+        // (largest tau first) until one passes Armijo, so the accepted tau and
+        // vertices are those of the one-at-a-time search.
+        const int32_t K = o->trials < kMaxTrials ? o->trials : kMaxTrials;
+        TPE_TRY(ensure(ctx, ctx->trial_raw, sizeof(double) * (size_t)m * K));
+        TPE_TRY(ensure(ctx, ctx->trial_cur, sizeof(double) * (size_t)m * K));
+        TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * 600));
+        double* d_taus = ctx->scalars.as<double>() + 560;
+        double* braw = ctx->trial_raw.as<double>();
+        double* bcur = ctx->trial_cur.as<double>();
+        while (tau >= o->tau_min) {
+            double taus[kMaxTrials];
+            int32_t nk = 0;
+            for (double t = tau; nk < K && t >= o->tau_min; t *= o->shrink) taus[nk++] = t;
+            TPE_CUDA_TRY(cudaMemcpyAsync(d_taus, taus, sizeof(double) * nk, cudaMemcpyHostToDevice,
+                                         ctx->stream));
+            { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+            step_batch_kernel<<<dim3((unsigned)((m + 255) / 256), (unsigned)nk), 256, 0,
+                                ctx->stream>>>(d_pos, dir, d_taus, m, braw); }
+            TPE_CUDA_TRY(cudaGetLastError());
+            int32_t okv[kMaxTrials], itv[kMaxTrials];
+            double pnv[kMaxTrials];
+            {
+                Timer tp(ctx, timings, TPE_PHASE_PROJECTION);
+                TPE_TRY(project_batch_dev(ctx, braw, nk, S, o, bcur, okv, itv, pnv, timings));
+            }
+            for (int32_t a = 0; a < nk; a++) {
+                double* ca = bcur + (size_t)a * m;
+                int64_t bad = 0;
+                if (okv[a]) TPE_TRY(count_nonfinite(ctx, m, ca, &bad));
+                if (okv[a] && !bad) {
+                    double e1 = 0.0;
+                    TPE_TRY(objective(ctx, ca, o, pen, &e1, timings));
+                    trials++;
+                    if (isfinite(e1) && e1 <= e0 - o->c1 * taus[a] * slope) {
+                        st->accepted = 1;
+                        st->reason = TPE_REASON_NONE;
+                        st->tau = taus[a];
+                        st->energy = e1;
+                        st->projection_iterations = itv[a];
+                        st->projection_phi_norm = pnv[a];
+                        st->trials_evaluated = trials;
+                        TPE_CUDA_TRY(cudaMemcpyAsync(d_out, ca, sizeof(double) * m,
+                                                     cudaMemcpyDeviceToDevice, ctx->stream));
+                        return TPE_OK;
+                    }
+                    lastReason = TPE_REASON_ARMIJO_FAILED;
+                } else {
+                    lastReason = TPE_REASON_PROJECTION_FAILED;
+                }
+            }
+            tau = taus[nk - 1] * o->shrink;
+        }
+        st->reason = lastReason;
+        st->trials_evaluated = trials;
+        return TPE_OK;
+    }
     while (tau >= o->tau_min) {
         { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
         step_kernel<<<(unsigned)((m + 255) / 256), 256, 0, ctx->stream>>>(d_pos, dir, tau, m, raw); }
@@ -847,7 +1055,7 @@ void tpe_default_step_opts(tpe_step_opts* o) {
     o->proj_tol_rel = 1e-4;
     o->proj_max_iter = 8;
     o->precision = TPE_PRECISION_FP64;
-    o->trials = 1;
+    o->trials = 8;
     o->refine_max_iter = 30;
     o->refine_tol = 1e-12;
 }

@@ -69,8 +69,15 @@ __device__ void block_reduce(double (&v)[N], bool is_max_last) {
 // One CTA per block: phi rows, and ns[2b] = ||phi_b||^2, ns[2b+1] = scale_b.
 __global__ void __launch_bounds__(kBS)
 phi_kernel(const double* __restrict__ pos, const int2* __restrict__ edges, int32_t E, int32_t V,
-           const DevBlock* __restrict__ blocks, double* __restrict__ phi, double* __restrict__ ns) {
+           const DevBlock* __restrict__ blocks, double* __restrict__ phi, double* __restrict__ ns,
+           int64_t pos_stride, const int32_t* __restrict__ idx, int32_t k) {
     const DevBlock B = blocks[blockIdx.x];
+    // batched form: position set idx[y] (or y), outputs of row y
+    if (gridDim.y > 1 || idx) {
+        pos += (idx ? idx[blockIdx.y] : (int32_t)blockIdx.y) * pos_stride;
+        phi += (size_t)blockIdx.y * k;
+        ns += (size_t)blockIdx.y * 2 * gridDim.x;
+    }
     if (B.kind == TPE_BLOCK_BARYCENTER) {
         double v[5] = {0, 0, 0, 0, 0};  // phi x,y,z, L, R(max)
         for (int32_t I = threadIdx.x; I < E; I += kBS) {
@@ -349,6 +356,18 @@ int32_t upload_set(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, int
     return TPE_OK;
 }
 
+int32_t eval_constraints_batch(tpe_ctx* ctx, const double* d_pos, int64_t stride,
+                               const int32_t* d_idx, int32_t n, int32_t nblocks, int32_t k,
+                               double* d_phi, double* d_ns) {
+    if (nblocks == 0 || n == 0) return TPE_OK;
+    KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+    phi_kernel<<<dim3((unsigned)nblocks, (unsigned)n), kBS, 0, ctx->stream>>>(
+        d_pos, ctx->d_edges.as<int2>(), ctx->E, ctx->V, ctx->con_blocks.as<DevBlock>(), d_phi,
+        d_ns, stride, d_idx, k);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
 int32_t eval_constraints(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k,
                          double* d_C, std::vector<double>& phi, std::vector<double>& ns) {
     const int32_t V = ctx->V, E = ctx->E;
@@ -360,7 +379,8 @@ int32_t eval_constraints(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int
     double* dns = dphi + k;
     { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
     phi_kernel<<<nblocks, kBS, 0, ctx->stream>>>(d_pos, ctx->d_edges.as<int2>(), E, V,
-                                                 ctx->con_blocks.as<DevBlock>(), dphi, dns); }
+                                                 ctx->con_blocks.as<DevBlock>(), dphi, dns, 0,
+                                                 nullptr, k); }
     TPE_CUDA_TRY(cudaGetLastError());
     if (d_C) {
         TPE_CUDA_TRY(cudaMemsetAsync(d_C, 0, sizeof(double) * (size_t)k * 3 * V, ctx->stream));

@@ -596,10 +596,17 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     int32_t* d_err = d_bad + 1;
     double* d = ctx->mx_d.as<double>();
     float* S = ctx->mx_S.as<float>();
-    tc::SplitMat Sm;  // the trailing matrix as a plain FP32 GEMM output
-    Sm.hi = S;
-    Sm.lo = nullptr;
-    Sm.rows = Sm.cols = Sm.ld = Vp;
+    tc::SplitMat& Sm = mf.S;  // the trailing matrix as a plain FP32 GEMM output
+    if (Sm.hi != S || Sm.rows != Vp) {
+        Sm.hi = S;
+        Sm.lo = nullptr;
+        Sm.rows = Sm.cols = Sm.ld = Vp;
+        if (!tc::make_maps(Sm)) {
+            Sm.hi = nullptr;
+            set_error(ctx, TPE_ERR_CUDA, "cuTensorMapEncodeTiled failed for the FP32 trailing matrix");
+            return TPE_ERR_CUDA;
+        }
+    }
     const int nb = Vp / kT;
     const size_t potrf_smem = sizeof(float) * (2 * kT * kLd + 96 * kPl + kT);
     TPE_CUDA_TRY(cudaFuncSetAttribute(potrf128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

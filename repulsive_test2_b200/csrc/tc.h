@@ -25,9 +25,11 @@ struct SplitMat {
     float* lo = nullptr;  // null for a plain FP32 output matrix (gemm_nt's C only)
     int32_t rows = 0, cols = 0, ld = 0;
     CUtensorMap map_hi, map_lo;  // 128 x 32 boxes, 128B swizzle
+    bool maps_ok = false;
 };
 
-// Encodes the two tensor maps of m (host only). Returns false on failure.
+// Encodes the tensor maps of m (host only; hi only when lo is null). Returns
+// false on failure.
 bool make_maps(SplitMat& m);
 
 enum : int32_t {

@@ -36,6 +36,7 @@ struct KParams {
     float* c_hi;
     float* c_lo;
     int32_t ldc;
+    int32_t tma_epi;  // 0: register epilogue; 1: TMA store (beta 0); 2: TMA reduce-add (beta 1, plain C)
     int32_t* err;
 };
 
@@ -103,6 +104,23 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, uint32_t src, int32_t x,
+                                             int32_t y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                     (uint64_t)map),
+                 "r"(src), "r"(x), "r"(y)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, uint32_t src, int32_t x,
+                                                  int32_t y) {
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+            (uint64_t)map),
+        "r"(src), "r"(x), "r"(y)
+        : "memory");
+}
+
 // Shared-memory matrix descriptor: K-major operand, 128B swizzle, 8-row groups
 // 1024 bytes apart (SBO), descriptor version 1 (bit 46), layout 2 = SWIZZLE_128B.
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
@@ -147,6 +165,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 __global__ void __launch_bounds__(128, 1)
 gemm_nt_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__ CUtensorMap a_lo,
                const __grid_constant__ CUtensorMap b_hi, const __grid_constant__ CUtensorMap b_lo,
+               const __grid_constant__ CUtensorMap c_hi, const __grid_constant__ CUtensorMap c_lo,
                const KParams P) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -254,9 +273,57 @@ gemm_nt_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__
     __syncthreads();
 
     bool ok = mbar_wait(done, 0, P.err);
-    ok = __all_sync(0xffffffffu, ok) && !*aborted;
+    ok = __syncthreads_and(ok && !*aborted) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok) {
+    if (ok && P.tma_epi) {
+        // Stage the tile in the (now idle) pipeline buffers in the 128B-swizzled
+        // box layout of the C tensor maps (4 boxes of 128 rows x 32 columns; a
+        // second set for lo), then one thread stores or reduce-adds the boxes.
+        const bool split_out = P.c_lo != nullptr;
+        const int r = warp * 32 + lane;
+        const float alpha = g.alpha;
+        for (int b = 0; b < 4; b++) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(32 * b), v);
+            uint8_t* row_hi = smem + b * kTileBytes + r * 128;
+            uint8_t* row_lo = smem + 4 * kTileBytes + b * kTileBytes + r * 128;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int pq = (q ^ (r & 7)) * 16;
+                float4 y = make_float4(alpha * v[4 * q], alpha * v[4 * q + 1], alpha * v[4 * q + 2],
+                                       alpha * v[4 * q + 3]);
+                if (split_out) {
+                    float4 h, l;
+                    split(y.x, h.x, l.x);
+                    split(y.y, h.y, l.y);
+                    split(y.z, h.z, l.z);
+                    split(y.w, h.w, l.w);
+                    *reinterpret_cast<float4*>(row_hi + pq) = h;
+                    *reinterpret_cast<float4*>(row_lo + pq) = l;
+                } else {
+                    *reinterpret_cast<float4*>(row_hi + pq) = y;
+                }
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int32_t x0 = g.c_c0 + z * g.c_zc + tj * kBN, y0 = g.c_r0 + z * g.c_zr + ti * kBM;
+            for (int b = 0; b < 4; b++) {
+                const uint32_t src = smem_u32(smem + b * kTileBytes);
+                if (P.tma_epi == 2)
+                    tma_reduce_add_2d(&c_hi, src, x0 + 32 * b, y0);
+                else
+                    tma_store_2d(&c_hi, src, x0 + 32 * b, y0);
+            }
+            if (split_out)
+                for (int b = 0; b < 4; b++)
+                    tma_store_2d(&c_lo, smem_u32(smem + 4 * kTileBytes + b * kTileBytes),
+                                 x0 + 32 * b, y0);
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        }
+    } else if (ok) {
         const int row = ti * kBM + warp * 32 + lane;
         const bool rin = row < g.M;
         const int32_t cr = g.c_r0 + z * g.c_zr + (rin ? row : 0);
@@ -369,10 +436,14 @@ bool encode(CUtensorMap* map, float* base, int32_t rows, int32_t cols, int32_t l
 }  // namespace
 
 bool make_maps(SplitMat& m) {
-    if (!m.hi || !m.lo || m.rows <= 0 || m.cols <= 0 || m.ld % 32 != 0 || m.cols > m.ld) return false;
+    m.maps_ok = false;
+    if (!m.hi || m.rows <= 0 || m.cols <= 0 || m.ld % 32 != 0 || m.cols > m.ld) return false;
     if (((uintptr_t)m.hi | (uintptr_t)m.lo) & 127) return false;
-    return encode(&m.map_hi, m.hi, m.rows, m.cols, m.ld) &&
-           encode(&m.map_lo, m.lo, m.rows, m.cols, m.ld);
+    if (!encode(&m.map_hi, m.hi, m.rows, m.cols, m.ld)) return false;
+    if (m.lo && !encode(&m.map_lo, m.lo, m.rows, m.cols, m.ld)) return false;
+    if (!m.lo) m.map_lo = m.map_hi;
+    m.maps_ok = true;
+    return true;
 }
 
 cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const GemmArgs& g,
@@ -406,7 +477,17 @@ cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const Gem
     P.c_lo = C.lo;
     P.ldc = C.ld;
     P.err = err;
-    gemm_nt_kernel<<<grid, 128, kSmemBytes, stream>>>(A.map_hi, A.map_lo, B.map_hi, B.map_lo, P);
+    // TMA epilogue for whole tiles: a store when beta == 0, a reduce-add into a
+    // plain C when beta == 1; anything else takes the register epilogue.
+    P.tma_epi = 0;
+    if (C.maps_ok && g.M % kBM == 0 && g.N % kBN == 0 && ((g.c_c0 | g.c_zc) & 3) == 0) {
+        if (g.beta == 0.0f)
+            P.tma_epi = 1;
+        else if (g.beta == 1.0f && !C.lo)
+            P.tma_epi = 2;
+    }
+    gemm_nt_kernel<<<grid, 128, kSmemBytes, stream>>>(A.map_hi, A.map_lo, B.map_hi, B.map_lo,
+                                                      C.map_hi, C.map_lo, P);
     return cudaGetLastError();
 }
 

@@ -42,6 +42,8 @@ constexpr int kNB = 64;
 // Most right-hand sides (3 per constraint row, +3 for b) the mixed solve takes
 // at factor time; larger sets use the FP64 factorization.
 constexpr int kMixedMaxRhs = 48;
+// Most step sizes one batched line-search launch projects together.
+constexpr int kMaxTrials = 16;
 
 // Everything the structured saddle solve keeps between the factorization and
 // later solves: the frozen operator of optimizer.ts's 'frozen' projection.
@@ -76,6 +78,7 @@ struct MixedFactor {
     int V = 0, Vp = 0;
     double rho = 0.0;
     tc::SplitMat L, Z, W, T;
+    tc::SplitMat S;  // plain FP32 trailing matrix (hi only)
 };
 
 struct DevBlock {
@@ -115,6 +118,7 @@ struct tpe_ctx {
     tpe::DevBuf con_C, con_Y, con_phi, con_blocks, con_ell0, con_red;
     tpe::DevBuf rhs, sol, tmp, solve_scratch;
     tpe::DevBuf status;                     // device-side int flags
+    tpe::DevBuf trial_raw, trial_cur;       // batched line-search trials (K x 3V each)
     tpe::SaddleOp op;
     // mixed-precision factor (mixed.cu)
     tpe::DevBuf mx_d, mx_dinv, mx_S, mx_Lhi, mx_Llo, mx_Zhi, mx_Zlo, mx_Whi, mx_Wlo, mx_Thi, mx_Tlo,
@@ -213,6 +217,12 @@ int32_t upload_set(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, int
 // (k x 3V, device) when d_C != nullptr.
 int32_t eval_constraints(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k,
                          double* d_C, std::vector<double>& phi, std::vector<double>& norm_scale);
+
+// Phi (d_phi: n x k) and per-block {norm^2, scale} (d_ns: n x 2 nblocks), on the
+// device, for the position sets pos + idx[q] * stride, q < n (idx on the device).
+int32_t eval_constraints_batch(tpe_ctx* ctx, const double* d_pos, int64_t stride,
+                               const int32_t* d_idx, int32_t n, int32_t nblocks, int32_t k,
+                               double* d_phi, double* d_ns);
 
 // ---- small device helpers (dense.cu) --------------------------------------
 int32_t interleaved_to_block(tpe_ctx* ctx, const double* d_v3, double* d_flat, int32_t V);
