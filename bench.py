@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="repulsive", choices=["repulsive", "reference"])
     p.add_argument("--V", type=int, default=8192)
-    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work")
     return p.parse_args()
@@ -153,6 +153,14 @@ def ncu_traffic(kernel):
 
 # ---- CPU baseline: the oracle (C restatement of the reference's TS path) -------------
 
+# Line-search work of one step on this workload, as the GPU FP64 step does it
+# from the initial curve: 7 step sizes tried (tau = 1 .. 2^-6), the first 5
+# projections fail at the 8-correction cap, the last 2 converge in 3 and are
+# the 2 energy evaluations (E0 comes in as energyBefore).
+LS_ENERGIES = 2
+LS_SOLVES = 5 * 8 + 2 * 3
+
+
 def cpu_step_estimate(v, e, blocks, step_stats, budget_s):
     """Times bounded samples of the oracle's step at full size and scales each
     phase by its exact operation count: gradient, energy and Gram assembly over a
@@ -210,20 +218,27 @@ def cpu_step_estimate(v, e, blocks, step_stats, budget_s):
         ns = int(ns * 1.6)
     t_fac = tf * (n / ns) ** 3
     t_sol = ts * (n / ns) ** 2
-    trials = max(1, int(step_stats.get("trials", 1)))
-    iters = max(0, int(step_stats.get("projection_iterations", 1) or 0))
-    # E0 + one energy per trial; one LDL^T solve for g~ plus one per projection
-    # iterate of every trial (frozen); the structured residual is an O(n^2) matvec.
-    total = t_grad + t_en * (1 + trials) + t_asm + t_fac + t_sol * (1 + trials * iters) + t_sol
+    energies = int(step_stats.get("energies", LS_ENERGIES))
+    solves = int(step_stats.get("solves", LS_SOLVES))
+    # the line search's energies, one LDL^T solve for g~ plus one per projection
+    # correction (frozen), and the structured residual (an O(n^2) matvec ~ a solve)
+    total = t_grad + t_en * energies + t_asm + t_fac + t_sol * (1 + solves) + t_sol
     desc = (f"oracle (C restatement of the reference TS path, 1 thread), V={V}: gradient {r_g} of {E} "
-            f"edge rows x{E / r_g:.0f}, energy {r_e} rows x{E / r_e:.0f} x(1+{trials} trials), "
-            f"assembly {r_a} rows x{E / r_a:.0f}, Bunch-Kaufman LDL^T of order {ns} scaled to n={n} "
-            f"by (n/ns)^3, its solve by (n/ns)^2")
+            f"edge rows x{E / r_g:.0f}, energy {r_e} rows x{E / r_e:.0f} x{energies} line-search "
+            f"evaluations, assembly {r_a} rows x{E / r_a:.0f}, Bunch-Kaufman LDL^T of order {ns} scaled "
+            f"to n={n} by (n/ns)^3, its solve by (n/ns)^2 x{1 + solves}")
     return total, desc, {"grad_s": t_grad, "energy_s": t_en, "assemble_s": t_asm, "factor_s": t_fac,
                          "solve_s": t_sol}
 
 
 # ---- our arm ---------------------------------------------------------------------------
+
+def step_opts(T, precision):
+    """mixed+batched: FP32 tensor-core factor + FP64 CG, 8 step sizes projected per
+    batch; plain FP64: FP64 factorization, one step size at a time."""
+    return T._opts({"projectionMode": "frozen", "precision": precision,
+                    "trials": 8 if precision == "mixed" else 1})
+
 
 def run_repulsive(args):
     import torch
@@ -247,66 +262,95 @@ def run_repulsive(args):
     ctx.topology(v, e)
     lib = ctx.lib
     arr, keep = abi.make_set(blocks)
-    o = T._opts({"projectionMode": "frozen", "precision": args.precision})
     st = abi.tpe_step_stats()
-    d_in = torch.from_numpy(v.copy()).to(dev)
-    d_out = torch.empty_like(d_in)
     stream = torch.cuda.ExternalStream(lib.tpe_stream(ctx.ptr), device=dev)
+    params = abi.tpe_params(3.0, 6.0, 1e-10)
+    e_init = C.c_double(0.0)
+    ctx.check(lib.tpe_energy(ctx.ptr, np.ascontiguousarray(v).ctypes.data_as(abi.dp), C.byref(params),
+                             C.byref(e_init)), "tpe_energy")
+    E0 = e_init.value
+    d_init = torch.from_numpy(v.copy()).to(dev)
+    bufs = [torch.empty_like(d_init), torch.empty_like(d_init)]
 
-    def dev_step():
-        rc = lib.tpe_sobolev_step_device(ctx.ptr, d_in.data_ptr(), arr, len(blocks), C.byref(o),
-                                         d_out.data_ptr(), C.byref(st), None)
-        ctx.check(rc, "tpe_sobolev_step_device")
+    def dev_trajectory(o, nsteps, log=None):
+        """nsteps descent steps from the initial curve; step i starts at the
+        output of step i-1 with its energy as energyBefore (the app's loop)."""
+        bufs[0].copy_(d_init)
+        cur, nxt = 0, 1
+        e_before = E0
+        for _ in range(nsteps):
+            o.has_energy_before = 1
+            o.energy_before = e_before
+            rc = lib.tpe_sobolev_step_device(ctx.ptr, bufs[cur].data_ptr(), arr, len(blocks), C.byref(o),
+                                             bufs[nxt].data_ptr(), C.byref(st), None)
+            ctx.check(rc, "tpe_sobolev_step_device")
+            if log is not None:
+                log.append({"tau": st.tau, "trials": st.trials_evaluated, "accepted": st.accepted,
+                            "refine": st.refine_iterations, "energy": st.energy})
+            if st.accepted:
+                cur, nxt = nxt, cur
+                e_before = st.energy
 
-    for _ in range(args.warmup):
-        dev_step()
-    torch.cuda.synchronize(dev)
-    if dist:
-        dist.barrier()
-    lib.tpe_profile(ctx.ptr, 1)
-    with ClockSampler(local) as clk:
+    def timed(o, nsteps, log=None, profile=False):
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        if profile:
+            lib.tpe_profile(ctx.ptr, 1)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(dev)
         t0.record(stream)
-        for _ in range(args.steps):
-            dev_step()
+        dev_trajectory(o, nsteps, log)
         t1.record(stream)
         torch.cuda.synchronize(dev)
-    ms = t0.elapsed_time(t1)
-    kms = (C.c_double * len(abi.KGROUPS))()
-    kl = (C.c_int64 * (len(abi.KGROUPS) + 1))()
-    lib.tpe_profile_read(ctx.ptr, kms, kl)
-    lib.tpe_profile(ctx.ptr, 0)
-    step_info = {"trials": st.trials_evaluated, "projection_iterations": st.projection_iterations,
-                 "tau": st.tau, "accepted": st.accepted, "energy_before": st.energy_before,
-                 "energy_after": st.energy}
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = t0.elapsed_time(t1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    o_mix = step_opts(T, args.precision)
+    o_64 = step_opts(T, "fp64")
+    for _ in range(args.warmup):
+        dev_trajectory(o_mix, 1)
+        dev_trajectory(o_64, 1)
+    log_mix, log_64 = [], []
+    with ClockSampler(local) as clk:
+        ms = timed(o_mix, args.steps, log_mix, profile=True)
+        kms = (C.c_double * len(abi.KGROUPS))()
+        kl = (C.c_int64 * (len(abi.KGROUPS) + 1))()
+        lib.tpe_profile_read(ctx.ptr, kms, kl)
+        lib.tpe_profile(ctx.ptr, 0)
+        ms64 = timed(o_64, args.steps, log_64)
 
     # e2e: the public host-buffer API (pinned host in/out, copies inside the region)
-    pin_in = torch.from_numpy(v.copy()).pin_memory()
-    pin_out = torch.empty_like(pin_in).pin_memory()
-    vin = pin_in.numpy()
-    vout = pin_out.numpy()
-    inp = vin.ctypes.data_as(abi.dp)
-    outp = vout.ctypes.data_as(abi.dp)
+    pin = [torch.from_numpy(v.copy()).pin_memory(), torch.empty_like(torch.from_numpy(v)).pin_memory()]
+    hp = [pin[0].numpy().ctypes.data_as(abi.dp), pin[1].numpy().ctypes.data_as(abi.dp)]
 
-    def host_step():
-        rc = lib.tpe_sobolev_step(ctx.ptr, inp, arr, len(blocks), C.byref(o), outp, C.byref(st), None, None)
-        ctx.check(rc, "tpe_sobolev_step")
+    def host_trajectory(o, nsteps):
+        pin[0].copy_(torch.from_numpy(v))
+        cur, nxt = 0, 1
+        e_before = E0
+        for _ in range(nsteps):
+            o.has_energy_before = 1
+            o.energy_before = e_before
+            rc = lib.tpe_sobolev_step(ctx.ptr, hp[cur], arr, len(blocks), C.byref(o), hp[nxt], C.byref(st),
+                                      None, None)
+            ctx.check(rc, "tpe_sobolev_step")
+            if st.accepted:
+                cur, nxt = nxt, cur
+                e_before = st.energy
 
-    host_step()
+    host_trajectory(o_mix, 1)
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        host_step()
+    host_trajectory(o_mix, args.steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = e0.elapsed_time(e1)
@@ -314,6 +358,27 @@ def run_repulsive(args):
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
+
+    # accuracy of the mixed step against the FP64 step from the initial curve
+    acc = {}
+    if rank == 0:
+        res = {}
+        for name, o in (("mixed", step_opts(T, args.precision)), ("fp64", step_opts(T, "fp64"))):
+            res[name] = T.sobolevStepSet(v, e, None, blocks,
+                                         {"projectionMode": "frozen", "precision": name if name == "fp64" else args.precision,
+                                          "trials": o.trials, "collectField": True})
+        rm, rf = res["mixed"], res["fp64"]
+        gm, gf = rm["descentField"], rf["descentField"]
+        acc = {"energy_rel_err": abs(rm["energy"] - rf["energy"]) / abs(rf["energy"]),
+               "projected_gradient_rel_err": float(np.linalg.norm(gm - gf) / np.linalg.norm(gf)),
+               "vertices_rel_err": float(np.linalg.norm(rm["vertices"] - rf["vertices"]) /
+                                         np.linalg.norm(rf["vertices"])),
+               "tau_equal": rm["stats"]["tau"] == rf["stats"]["tau"],
+               "saddle_residual": rm["stats"]["residual"],
+               "cg_iterations": rm["stats"]["refineIterations"],
+               "note": "energy_rel_err: the accepted energy after one step from the initial curve, "
+                       "mixed vs FP64 (both evaluate it with the FP64 pair kernels; FP32 pair terms would "
+                       "give 1.5e-7 here); the mixed mode differs from FP64 only in the saddle solve"}
 
     if rank != 0:
         if dist:
@@ -329,30 +394,37 @@ def run_repulsive(args):
     peaks = measured_peaks()
     fp64_peak = fp64_gemm_peak(torch, dev)
     steps = args.steps
-    # algorithmic work per launch of the dominant group
-    if dom == "cholesky":
-        per_launch_flop = V ** 3 / 3.0  # one Cholesky of A_rho per step
-        n_launch = steps
-        roof = {"bound": "tensor", "unit": "TFLOP/s", "peak": fp64_peak,
-                "peak_source": "cuBLAS FP64 GEMM measured in this run (no FP64 entry in MEASURED_PEAKS.json)",
-                "kernel": "cholesky (potrf_diag+trsm_panel+syrk_update), per factorization",
-                "work_per_launch": f"V^3/3 = {per_launch_flop:.3e} flop"}
-        achieved = per_launch_flop * n_launch / (ms_g[dom] * 1e-3) / 1e12
-    elif dom in ("gradient", "energy", "pair_weights"):
-        P = len(e) * (len(e) - 3)
+    P = len(e) * (len(e) - 3)
+    if dom in ("gradient", "energy", "pair_weights"):
         fl = {"gradient": 2 * 4 * 110, "energy": 4 * 34, "pair_weights": 4 * 45}[dom]
         per_launch_flop = P * fl
         n_launch = max(1, nl[dom] // {"gradient": 2, "energy": 2, "pair_weights": 1}[dom])
         roof = {"bound": "tensor", "unit": "TFLOP/s", "peak": fp64_peak,
-                "peak_source": "cuBLAS FP64 GEMM measured in this run (FP64 pipe reference)",
+                "peak_source": "cuBLAS FP64 GEMM measured in this run (the FP64 pipe; MEASURED_PEAKS.json "
+                               "lists HBM and bf16 only)",
                 "kernel": dom, "work_per_launch": f"{fl} flop x {P} ordered pairs"}
         achieved = per_launch_flop * n_launch / (ms_g[dom] * 1e-3) / 1e12
+    elif dom == "cholesky":
+        per_launch_flop = V ** 3 / 3.0
+        n_launch = steps
+        tf32 = peaks.get("bf16_tflops", 1590.0) / 2.0
+        if args.precision == "mixed":
+            roof = {"bound": "tensor", "unit": "TFLOP/s", "peak": tf32 / 3.0,
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops / 2 (TF32) / 3 (3xTF32 products per "
+                                   "algorithmic FMA)",
+                    "kernel": "FP32 Cholesky of the scaled A_rho (potrf128 + tcgen05 3xTF32 GEMMs), per "
+                              "factorization", "work_per_launch": f"V^3/3 = {per_launch_flop:.3e} flop"}
+        else:
+            roof = {"bound": "tensor", "unit": "TFLOP/s", "peak": fp64_peak,
+                    "peak_source": "cuBLAS FP64 GEMM measured in this run",
+                    "kernel": "FP64 Cholesky (DMMA)", "work_per_launch": f"V^3/3 = {per_launch_flop:.3e} flop"}
+        achieved = per_launch_flop * n_launch / (ms_g[dom] * 1e-3) / 1e12
     else:
-        per_launch_bytes = 8.0 * V * V * 2
+        per_launch_bytes = 8.0 * V * V
         n_launch = max(1, nl[dom])
         roof = {"bound": "hbm", "unit": "GB/s", "peak": peaks.get("hbm_gbs", 6650.0),
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
-                "kernel": dom, "work_per_launch": "16 V^2 bytes"}
+                "kernel": dom, "work_per_launch": "8 V^2 bytes"}
         achieved = per_launch_bytes * n_launch / (ms_g[dom] * 1e-3) / 1e9
     roof["achieved"] = achieved
     roof["frac"] = achieved / roof["peak"] if roof["peak"] else None
@@ -362,7 +434,15 @@ def run_repulsive(args):
     roof["group_launches"] = {g: int(nl[g]) for g in groups}
 
     value = world * steps / (ms * 1e-3)
+    value64 = world * steps / (ms64 * 1e-3)
     e2e_value = world * steps / (e2e_ms * 1e-3)
+
+    def traj(log):
+        return {"accepted": sum(x["accepted"] for x in log),
+                "energy_evaluations": sum(x["trials"] for x in log),
+                "taus": [x["tau"] for x in log], "cg_iterations": [x["refine"] for x in log],
+                "energy_last": log[-1]["energy"] if log else None}
+
     out = {
         "metric": METRIC,
         "value": value,
@@ -374,13 +454,21 @@ def run_repulsive(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32-mixed",
+        "dtype": "f64+tf32x3" if args.precision == "mixed" else "f64",
         "data": "synthetic: seeded random-walk knot (splitmix64/Box-Muller), no dataset",
-        "config": {"workload": f"random-walk closed knot V=E={V}, [barycenter,totalLength], frozen projection, "
-                               "analytical dE, one sobolevStepSet per step from the same input",
-                   "V": V, "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "working set larger than L2 (A and L are 537 MB each, pair matrix 1.07 GB)"},
-        "step": step_info,
+        "config": {"workload": f"random-walk closed knot V=E={V}, [barycenter,totalLength] frozen at the "
+                               "initial curve, frozen projection, analytical dE; a descent trajectory of "
+                               "`steps` steps from the initial curve, each step starting at the previous "
+                               "output with its energy as energyBefore (the app's loop)",
+                   "V": V, "precision": args.precision,
+                   "line_search": "8 step sizes projected per batch" if args.precision == "mixed" else "sequential",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "working set larger than L2 (A is 537 MB, the FP32 factor and its inverse 1.6 GB)"},
+        "fp64": {"value": value64, "unit": "steps/s", "ms_per_step": ms64 / steps,
+                 "config": "plain FP64 GPU step: FP64 Cholesky, one step size at a time", "trajectory": traj(log_64)},
+        "speedup_vs_fp64": value / value64,
+        "accuracy_vs_fp64": acc,
+        "trajectory": traj(log_mix),
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 8 * 3 * V,
                 "d2h_bytes_per_step": 8 * 3 * V},
@@ -388,7 +476,7 @@ def run_repulsive(args):
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline and world == 1:
-        t_cpu, desc, parts = cpu_step_estimate(v, e, blocks, step_info, args.cpu_budget)
+        t_cpu, desc, parts = cpu_step_estimate(v, e, blocks, {}, args.cpu_budget)
         out["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "steps/s", "cores": 1, "kind": "port",
                                "sample": desc, "phases_s": {k: round(x, 3) for k, x in parts.items()}}
     print(json.dumps(out), flush=True)
@@ -405,11 +493,11 @@ def run_reference(args):
     v, e, blocks = workload(args.V)
     per_step = max(2.0, min(30.0, 150.0 / max(1, args.steps)))
     # warm-up: one small sample (the CPU has no compile/caching stage to warm)
-    cpu_step_estimate(v, e, blocks, {"trials": 1, "projection_iterations": 1}, 1.0)
+    cpu_step_estimate(v, e, blocks, {}, 1.0)
     t_total = 0.0
     desc = ""
     for _ in range(args.steps):
-        t, desc, _parts = cpu_step_estimate(v, e, blocks, {"trials": 1, "projection_iterations": 1}, per_step)
+        t, desc, _parts = cpu_step_estimate(v, e, blocks, {}, per_step)
         t_total += t
     value = args.steps / t_total
     out = {
@@ -426,8 +514,9 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic: seeded random-walk knot (splitmix64/Box-Muller), no dataset",
-        "config": {"workload": f"random-walk closed knot V=E={args.V}, [barycenter,totalLength], frozen projection, "
-                               "analytical dE, one sobolevStepSet per step", "V": args.V},
+        "config": {"workload": f"random-walk closed knot V=E={args.V}, [barycenter,totalLength] frozen at the "
+                               "initial curve, frozen projection, analytical dE, one sobolevStepSet per step "
+                               "(energyBefore supplied)", "V": args.V},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
