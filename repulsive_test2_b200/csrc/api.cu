@@ -317,6 +317,44 @@ int32_t check_topology(tpe_ctx* ctx) {
     return TPE_OK;
 }
 
+// ---- gradient on the side stream ---------------------------------------------
+
+// Launches issued while in scope go to stream s (KernelScope events included).
+struct StreamSwap {
+    tpe_ctx* ctx;
+    cudaStream_t saved;
+    StreamSwap(tpe_ctx* c, cudaStream_t s) : ctx(c), saved(c->stream) { ctx->stream = s; }
+    ~StreamSwap() { ctx->stream = saved; }
+};
+
+// Launches the gradient prepared by step_impl on stream3 (after the work the
+// main stream has issued so far, i.e. after the assembly).
+int32_t launch_gradient(tpe_ctx* ctx) {
+    if (!ctx->grad_unlaunched) return TPE_OK;
+    ctx->grad_unlaunched = false;
+    TPE_CUDA_TRY(cudaEventRecord(ctx->ev_prep, ctx->stream));
+    TPE_CUDA_TRY(cudaStreamWaitEvent(ctx->stream3, ctx->ev_prep, 0));
+    {
+        StreamSwap sw(ctx, ctx->stream3);
+        TPE_TRY(energy_grad_fp64(ctx, ctx->grad_params[0], ctx->grad_params[1], ctx->grad_params[2],
+                                 nullptr, ctx->grad_dE));
+    }
+    TPE_CUDA_TRY(cudaEventRecord(ctx->ev_grad, ctx->stream3));
+    return TPE_OK;
+}
+
+// Joins the gradient launched on stream3 (step_impl) into the main stream and
+// finishes the right-hand side: penalty gradient, coordinate-block layout.
+int32_t finish_gradient(tpe_ctx* ctx) {
+    if (!ctx->grad_pending) return TPE_OK;
+    TPE_TRY(launch_gradient(ctx));
+    ctx->grad_pending = false;
+    TPE_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_grad, 0));
+    if (ctx->grad_pen)
+        TPE_TRY(penalty_gradient_dev(ctx, ctx->grad_pos, ctx->grad_pen, ctx->grad_dE, 1));
+    return interleaved_to_block(ctx, ctx->grad_dE, ctx->grad_flat, ctx->V);
+}
+
 // ---- saddle operator ----------------------------------------------------------
 
 // Factor A_rho and the Schur complement from ctx->mat_A (V x V) and ctx->con_C (k x 3V).
@@ -374,15 +412,22 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
     const int32_t rows = k + (b_flat ? 1 : 0);
     TPE_TRY(ensure(ctx, ctx->con_Y, sizeof(double) * (size_t)(rows > 0 ? rows : 1) * 3 * V));
     op.Y = ctx->con_Y.as<double>();
-    if (k > 0)
-        TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
     if (b_flat) {
         op.W = op.Y + (size_t)k * 3 * V;
         op.w_src = b_flat;
-        TPE_CUDA_TRY(cudaMemcpyAsync(op.W, b_flat, sizeof(double) * 3 * (size_t)V,
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
     }
+    // the right-hand sides, loaded right before the solves (b may still be in
+    // the making on another stream: finish_gradient joins it)
+    auto load_rhs = [&]() -> int32_t {
+        TPE_TRY(finish_gradient(ctx));
+        if (k > 0)
+            TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+        if (b_flat)
+            TPE_CUDA_TRY(cudaMemcpyAsync(op.W, b_flat, sizeof(double) * 3 * (size_t)V,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+        return TPE_OK;
+    };
     const int32_t nrhs = 3 * rows;
     if (o && o->precision == TPE_PRECISION_MIXED && nrhs <= kMixedMaxRhs) {
         // FP32 tensor-core factor as the preconditioner of an FP64 CG; the FP64
@@ -392,6 +437,7 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
         if (ok && nrhs > 0) {
             bool conv = false;
             int32_t it = 0;
+            TPE_TRY(load_rhs());
             TPE_TRY(mixed_solve(ctx, op.A, op.Y, op.Y, nrhs, o->refine_max_iter, o->refine_tol,
                                 &it, &conv));
             op.refine_iters = it;
@@ -401,12 +447,6 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
             op.mixed = true;
         } else {
             op.mixed_fallback = true;
-            if (k > 0)
-                TPE_CUDA_TRY(cudaMemcpyAsync(op.Y, op.C, sizeof(double) * (size_t)k * 3 * V,
-                                             cudaMemcpyDeviceToDevice, ctx->stream));
-            if (b_flat)
-                TPE_CUDA_TRY(cudaMemcpyAsync(op.W, b_flat, sizeof(double) * 3 * (size_t)V,
-                                             cudaMemcpyDeviceToDevice, ctx->stream));
         }
     }
     if (!op.mixed) {
@@ -418,6 +458,7 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
             *singular = true;
             return TPE_OK;
         }
+        TPE_TRY(load_rhs());
         for (int32_t r0 = 0; r0 < nrhs; r0 += 64) {
             const int32_t nr = (nrhs - r0) < 64 ? (nrhs - r0) : 64;
             TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, op.Y + (size_t)r0 * V, nr));
@@ -497,8 +538,11 @@ int32_t op_build(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k, 
     {
         Timer t(ctx, timings, TPE_PHASE_ASSEMBLEA);
         TPE_TRY(ensure(ctx, ctx->mat_A, sizeof(double) * (size_t)V * V));
-        TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
+        // the edge records of d_pos may already be in place (step_impl prepares
+        // them once for the gradient, which reads them concurrently)
+        if (!(ctx->grad_pending && ctx->grad_pos == d_pos)) TPE_TRY(edge_prep(ctx, d_pos, 1, eps, alpha));
         TPE_TRY(assemble_fp64(ctx, alpha, beta, eps, ctx->mat_A.as<double>(), nullptr, nullptr));
+        TPE_TRY(launch_gradient(ctx));
     }
     TPE_TRY(ensure(ctx, ctx->con_C, sizeof(double) * (size_t)(k > 0 ? k : 1) * 3 * V));
     std::vector<double> phi, ns;
@@ -1084,7 +1128,10 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
     int prio_lo = 0, prio_hi = 0;
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
+        cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->stream3, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_prep, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_grad, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;
         if (status) *status = TPE_ERR_CUDA;
         return nullptr;
@@ -1098,13 +1145,19 @@ void tpe_destroy(tpe_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
+    if (ctx->stream3) cudaStreamSynchronize(ctx->stream3);
     DevBuf* bufs[] = {&ctx->d_edges, &ctx->d_inc_off, &ctx->d_inc, &ctx->pos, &ctx->pos2,
                       &ctx->pos3, &ctx->edge_a, &ctx->edge_b, &ctx->grad, &ctx->edge_acc,
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
                       &ctx->flat3, &ctx->dir, &ctx->pairM, &ctx->edge_m, &ctx->mat_A, &ctx->mat_L,
                       &ctx->mat_Linv, &ctx->mat_B, &ctx->mat_B0, &ctx->con_C, &ctx->con_Y,
                       &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->rhs,
-                      &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status};
+                      &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status,
+                      &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
+                      &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,
+                      &ctx->mx_Wlo, &ctx->mx_Thi, &ctx->mx_Tlo, &ctx->mx_vec, &ctx->mx_part,
+                      &ctx->mx_Zd, &ctx->mx_Wd};
     for (DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     for (auto& p : ctx->prof_pending) {
@@ -1113,6 +1166,9 @@ void tpe_destroy(tpe_ctx* ctx) {
     }
     for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->fac_events) cudaEventDestroy(e);
+    if (ctx->ev_prep) cudaEventDestroy(ctx->ev_prep);
+    if (ctx->ev_grad) cudaEventDestroy(ctx->ev_grad);
+    if (ctx->stream3) cudaStreamDestroy(ctx->stream3);
     if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1424,21 +1480,44 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
     TPE_TRY(ensure(ctx, ctx->grad, sizeof(double) * m));
     double* dE = ctx->grad.as<double>();
     const bool pen = o->has_penalties && penalties_active(&o->penalties);
-    {
-        Timer t(ctx, timings, TPE_PHASE_DE);
-        if (o->mode == TPE_DE_FINITE_DIFF) {
-            TPE_TRY(gradient_fd_dev(ctx, P, o->alpha, o->beta, o->epsilon, o->h, dE));
-        } else {
-            TPE_TRY(edge_prep(ctx, P, 1, o->epsilon, o->alpha));
-            TPE_TRY(energy_grad_fp64(ctx, o->alpha, o->beta, o->epsilon, nullptr, dE));
-        }
-    }
-    if (pen) TPE_TRY(penalty_gradient_dev(ctx, P, &o->penalties, dE, 1));
     TPE_TRY(ensure(ctx, ctx->flat2, sizeof(double) * m));
-    TPE_TRY(interleaved_to_block(ctx, dE, ctx->flat2.as<double>(), V));
+    if (o->mode != TPE_DE_FINITE_DIFF && !timings) {
+        // The adjoint gradient (all SMs, FP64 pair work) does not depend on A:
+        // it runs on the low-priority stream3 while the main stream assembles
+        // and factors A_rho (a latency-bound chain); the solve joins it.
+        // op_build launches it right after the assembly (launch_gradient), so it
+        // overlaps the factorization and not the (equally compute-bound) Gram
+        // assembly.
+        TPE_TRY(edge_prep(ctx, P, 1, o->epsilon, o->alpha));
+        ctx->grad_unlaunched = true;
+        ctx->grad_params[0] = o->alpha;
+        ctx->grad_params[1] = o->beta;
+        ctx->grad_params[2] = o->epsilon;
+        ctx->grad_pending = true;
+        ctx->grad_pos = P;
+        ctx->grad_dE = dE;
+        ctx->grad_flat = ctx->flat2.as<double>();
+        ctx->grad_pen = pen ? &o->penalties : nullptr;
+    } else {
+        // sequential (finite differences, or the per-phase timing ledger)
+        {
+            Timer t(ctx, timings, TPE_PHASE_DE);
+            if (o->mode == TPE_DE_FINITE_DIFF) {
+                TPE_TRY(gradient_fd_dev(ctx, P, o->alpha, o->beta, o->epsilon, o->h, dE));
+            } else {
+                TPE_TRY(edge_prep(ctx, P, 1, o->epsilon, o->alpha));
+                TPE_TRY(energy_grad_fp64(ctx, o->alpha, o->beta, o->epsilon, nullptr, dE));
+            }
+        }
+        if (pen) TPE_TRY(penalty_gradient_dev(ctx, P, &o->penalties, dE, 1));
+        TPE_TRY(interleaved_to_block(ctx, dE, ctx->flat2.as<double>(), V));
+    }
     bool singular = false;
-    TPE_TRY(op_build(ctx, P, nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular, timings,
-                     ctx->flat2.as<double>(), o));
+    const int32_t bst = op_build(ctx, P, nblocks, S.k, o->alpha, o->beta, o->epsilon, &singular,
+                                 timings, ctx->flat2.as<double>(), o);
+    const int32_t fst = finish_gradient(ctx);  // joined even when the build returned early
+    TPE_TRY(bst);
+    TPE_TRY(fst);
     st->refine_iterations = ctx->op.mixed ? ctx->op.refine_iters : (ctx->op.mixed_fallback ? -1 : 0);
     TPE_TRY(ensure(ctx, ctx->sol, sizeof(double) * m));
     double* out = ctx->sol.as<double>();

@@ -13,9 +13,10 @@
 //      into one tcgen05 GEMM; W = Z^T is kept beside Z so every product is an
 //      A * B^T of row-major operands;
 //   4. used as the preconditioner M = Z^T Z = (L L^T)^{-1} of a block CG on
-//      S y = D b in FP64, x = D y. Z and W are copied to FP64 once (hi + lo is
-//      exact) and every product of the CG -- S p with the FP64 A, Z r, W u --
-//      runs on the FP64 tensor cores (mrhs_dmma_kernel).
+//      S y = D b in FP64, x = D y. Z and W are copied once to plain FP32
+//      (hi + lo is exact in FP32) and every product of the CG -- S p with the
+//      FP64 A, Z r and W u with the FP32 copies -- runs in FP64 arithmetic on
+//      the FP64 tensor cores (mrhs_dmma_kernel).
 // At V=8192 (kappa(A_rho) ~ 1e10, kappa(S) ~ 1e8) plain iterative refinement
 // with an FP32 factor diverges (kappa(S) * u32 > 1); CG with it reaches a 1e-13
 // relative residual in about 7 iterations. The FP64 path remains the fallback
@@ -134,7 +135,7 @@ __device__ __forceinline__ void tri_decode(int e, int& ti, int& tj) {
 // one block distance at a time, in the same 4 x 4 tiling. Reciprocal square
 // roots are the fast approximate ones: the factor is a preconditioner, CG
 // restores FP64 accuracy. *bad = 1 when a pivot is not positive and finite.
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, 2)
 potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __restrict__ Lhi,
                 float* __restrict__ Llo, float* __restrict__ Zhi, float* __restrict__ Zlo,
                 float* __restrict__ Whi, float* __restrict__ Wlo, int32_t* __restrict__ bad) {
@@ -380,9 +381,9 @@ __device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double
                  : "d"(a), "d"(b));
 }
 
-template <int TRI>
+template <int TRI, typename MT>
 __global__ void __launch_bounds__(256)
-mrhs_dmma_kernel(const double* __restrict__ M, int32_t ldm, int32_t n,
+mrhs_dmma_kernel(const MT* __restrict__ M, int32_t ldm, int32_t n,
                  const double* __restrict__ X, int32_t ldx, int32_t nr,
                  double* __restrict__ part) {
     __shared__ double xs[kMvChunk * kXs];
@@ -396,10 +397,10 @@ mrhs_dmma_kernel(const double* __restrict__ M, int32_t ldm, int32_t n,
     const int32_t ke = min(hi, ks + per);
     const int32_t row = r0 + warp * 8 + (lane >> 2);
     const bool rin = row < n;
-    const double* mrow = M + (size_t)(rin ? row : 0) * ldm;
+    const MT* mrow = M + (size_t)(rin ? row : 0) * ldm;
     const int m4 = (lane & 3) * 4;
     const int gq = lane >> 2;
-    const bool vec = (ldm & 1) == 0;
+    const bool vec = sizeof(MT) == 8 ? (ldm & 1) == 0 : (ldm & 3) == 0;
     double c0a = 0.0, c0b = 0.0, c1a = 0.0, c1b = 0.0;
     for (int32_t kc = ks; kc < ke; kc += kMvChunk) {
         const int32_t kn = min(kMvChunk, ke - kc);
@@ -413,15 +414,23 @@ mrhs_dmma_kernel(const double* __restrict__ M, int32_t ldm, int32_t n,
             const int32_t col = kc + g + m4;
             double a[4];
             if (rin && vec && col + 3 < ke) {
-                const double2 p0 = *reinterpret_cast<const double2*>(mrow + col);
-                const double2 p1 = *reinterpret_cast<const double2*>(mrow + col + 2);
-                a[0] = p0.x;
-                a[1] = p0.y;
-                a[2] = p1.x;
-                a[3] = p1.y;
+                if constexpr (sizeof(MT) == 8) {
+                    const double2 p0 = *reinterpret_cast<const double2*>(mrow + col);
+                    const double2 p1 = *reinterpret_cast<const double2*>(mrow + col + 2);
+                    a[0] = p0.x;
+                    a[1] = p0.y;
+                    a[2] = p1.x;
+                    a[3] = p1.y;
+                } else {
+                    const float4 p0 = *reinterpret_cast<const float4*>(mrow + col);
+                    a[0] = p0.x;
+                    a[1] = p0.y;
+                    a[2] = p0.z;
+                    a[3] = p0.w;
+                }
             } else {
 #pragma unroll
-                for (int t = 0; t < 4; t++) a[t] = (rin && col + t < ke) ? mrow[col + t] : 0.0;
+                for (int t = 0; t < 4; t++) a[t] = (rin && col + t < ke) ? (double)mrow[col + t] : 0.0;
             }
 #pragma unroll
             for (int s4 = 0; s4 < 4; s4++) {
@@ -457,27 +466,32 @@ __global__ void mrhs_reduce_kernel(const double* __restrict__ part, int32_t nspl
     Y[(size_t)c * ldx + i] = acc;
 }
 
-// FP64 copies of the inverse factor: Zd = Z on lower tiles (diagonal tiles
-// included, their upper parts are zero), Wd = W on upper tiles.
-__global__ void factor_to_f64_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
+// Plain FP32 copies of the inverse factor (hi + lo is exact in FP32): Zf = Z on
+// lower tiles (diagonal tiles included, their upper parts are zero), Wf = W
+// on upper tiles. The CG applies them with FP64 arithmetic.
+__global__ void factor_to_f32_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
                                      const float* __restrict__ whi, const float* __restrict__ wlo,
-                                     int32_t Vp, double* __restrict__ zd, double* __restrict__ wd) {
+                                     int32_t Vp, float* __restrict__ zf, float* __restrict__ wf) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (int64_t)Vp * Vp) return;
     const int32_t i = (int32_t)(t / Vp), j = (int32_t)(t % Vp);
     const int ti = i / kT, tj = j / kT;
-    if (ti >= tj) zd[t] = (double)zhi[t] + (double)zlo[t];
-    if (ti <= tj) wd[t] = (double)whi[t] + (double)wlo[t];
+    if (ti >= tj) zf[t] = zhi[t] + zlo[t];
+    if (ti <= tj) wf[t] = whi[t] + wlo[t];
 }
 
-// out[c] = sum_i a[c][i] b[c][i] w_i^2 (w null -> 1), one block per column.
-__global__ void col_dots_kernel(const double* __restrict__ a, const double* __restrict__ b,
-                                const double* __restrict__ w, int32_t Vp,
-                                double* __restrict__ out) {
+constexpr int kDotChunks = 32;
+
+// part[c][z] = sum over chunk z of a[c][i] b[c][i] w_i^2 (w null -> 1).
+__global__ void col_dots_part_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                     const double* __restrict__ w, int32_t Vp,
+                                     double* __restrict__ part) {
     __shared__ double red[8];
-    const int c = blockIdx.x;
+    const int c = blockIdx.y, z = blockIdx.x;
+    const int32_t len = (Vp + kDotChunks - 1) / kDotChunks;
+    const int32_t i0 = z * len, i1 = min(Vp, i0 + len);
     double acc = 0.0;
-    for (int32_t i = threadIdx.x; i < Vp; i += blockDim.x) {
+    for (int32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         double t = a[(size_t)c * Vp + i] * b[(size_t)c * Vp + i];
         if (w) t *= w[i] * w[i];
         acc += t;
@@ -488,8 +502,18 @@ __global__ void col_dots_kernel(const double* __restrict__ a, const double* __re
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) t += red[ww];
-        out[c] = t;
+        part[c * kDotChunks + z] = t;
     }
+}
+
+// out[c] = sum_z part[c][z] in a fixed order.
+__global__ void col_dots_final_kernel(const double* __restrict__ part, int32_t n,
+                                      double* __restrict__ out) {
+    const int c = threadIdx.x;
+    if (c >= n) return;
+    double t = 0.0;
+    for (int z = 0; z < kDotChunks; z++) t += part[c * kDotChunks + z];
+    out[c] = t;
 }
 
 // alpha_c = rz[c] / pq[c]; X += alpha P; R -= alpha Q
@@ -588,8 +612,8 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     TPE_TRY(make_split(ctx, ctx->mx_Zhi, ctx->mx_Zlo, Vp, Vp, mf.Z));
     TPE_TRY(make_split(ctx, ctx->mx_Whi, ctx->mx_Wlo, Vp, Vp, mf.W));
     if (Vp > kT) TPE_TRY(make_split(ctx, ctx->mx_Thi, ctx->mx_Tlo, Vp / 2, Vp / 2, mf.T));
-    TPE_TRY(ensure(ctx, ctx->mx_Zd, sizeof(double) * (size_t)Vp * Vp));
-    TPE_TRY(ensure(ctx, ctx->mx_Wd, sizeof(double) * (size_t)Vp * Vp));
+    TPE_TRY(ensure(ctx, ctx->mx_Zd, sizeof(float) * (size_t)Vp * Vp));
+    TPE_TRY(ensure(ctx, ctx->mx_Wd, sizeof(float) * (size_t)Vp * Vp));
     TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
     int32_t* d_bad = ctx->status.as<int32_t>() + 2;
     TPE_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 2 * sizeof(int32_t), st));
@@ -720,8 +744,8 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     }
     {
         KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
-        factor_to_f64_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(
-            mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, ctx->mx_Zd.as<double>(), ctx->mx_Wd.as<double>());
+        factor_to_f32_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(
+            mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, ctx->mx_Zd.as<float>(), ctx->mx_Wd.as<float>());
         TPE_CUDA_TRY(cudaGetLastError());
     }
     int32_t flags[2] = {0, 0};
@@ -749,7 +773,7 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
     *converged = true;
     *iters = 0;
     const size_t vec = (size_t)kMaxRhs * Vp;
-    TPE_TRY(ensure(ctx, ctx->mx_vec, sizeof(double) * (6 * vec + 8 * kMaxRhs)));
+    TPE_TRY(ensure(ctx, ctx->mx_vec, sizeof(double) * (6 * vec + 8 * kMaxRhs + kMaxRhs * kDotChunks)));
     constexpr int kSplit = 8;
     TPE_TRY(ensure(ctx, ctx->mx_part, sizeof(double) * (size_t)kSplit * kMaxRhs * Vp));
     double* X = ctx->mx_vec.as<double>();
@@ -764,10 +788,11 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
     double* rz[2] = {sc + 2 * kMaxRhs, sc + 3 * kMaxRhs};
     double* res2 = sc + 4 * kMaxRhs;
     double* bn2 = sc + 5 * kMaxRhs;
+    double* dpart = sc + 8 * kMaxRhs;  // kMaxRhs x kDotChunks partial dot products
     double* part = ctx->mx_part.as<double>();
     const double* d = ctx->mx_d.as<double>();
-    const double* Zd = ctx->mx_Zd.as<double>();
-    const double* Wd = ctx->mx_Wd.as<double>();
+    const float* Zf = ctx->mx_Zd.as<float>();
+    const float* Wf = ctx->mx_Wd.as<float>();
     std::vector<double> hres(kMaxRhs), hbn(kMaxRhs);
     int32_t max_iters = 0;
     const unsigned rb_V = (unsigned)((V + kMvRows - 1) / kMvRows);
@@ -778,10 +803,10 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
         // out = W (Z in): the preconditioner (L L^T)^{-1} of the scaled system
         auto precond = [&](const double* in, double* out) -> int32_t {
             KernelScope ks(ctx, TPE_KGROUP_TRSV, 4);
-            mrhs_dmma_kernel<1><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Zd, Vp, Vp, in, Vp, n, part);
+            mrhs_dmma_kernel<1, float><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Zf, Vp, Vp, in, Vp, n, part);
             mrhs_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, kSplit, Vp, Vp, n, nullptr, 0.0,
                                                                 nullptr, U);
-            mrhs_dmma_kernel<2><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Wd, Vp, Vp, U, Vp, n, part);
+            mrhs_dmma_kernel<2, float><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Wf, Vp, Vp, U, Vp, n, part);
             mrhs_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, kSplit, Vp, Vp, n, nullptr, 0.0,
                                                                 nullptr, out);
             TPE_CUDA_TRY(cudaGetLastError());
@@ -791,15 +816,16 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
         auto matvec = [&](const double* in, double* out) -> int32_t {
             KernelScope ks(ctx, TPE_KGROUP_OTHER, 3);
             cg_prep_kernel<<<n, 256, 0, st>>>(in, d, V, Vp, U, s_sum);
-            mrhs_dmma_kernel<0><<<dim3(rb_V, kSplit), 256, 0, st>>>(d_A, V, V, U, Vp, n, part);
+            mrhs_dmma_kernel<0, double><<<dim3(rb_V, kSplit), 256, 0, st>>>(d_A, V, V, U, Vp, n, part);
             mrhs_reduce_kernel<<<nblk((int64_t)n * V, 256), 256, 0, st>>>(part, kSplit, V, Vp, n, d,
                                                                            shift, s_sum, out);
             TPE_CUDA_TRY(cudaGetLastError());
             return TPE_OK;
         };
         auto dots = [&](const double* a, const double* b, const double* w, double* out) -> int32_t {
-            KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-            col_dots_kernel<<<n, 256, 0, st>>>(a, b, w, Vp, out);
+            KernelScope ks(ctx, TPE_KGROUP_OTHER, 2);
+            col_dots_part_kernel<<<dim3(kDotChunks, n), 256, 0, st>>>(a, b, w, Vp, dpart);
+            col_dots_final_kernel<<<1, 32, 0, st>>>(dpart, n, out);
             TPE_CUDA_TRY(cudaGetLastError());
             return TPE_OK;
         };

@@ -97,6 +97,16 @@ struct tpe_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;           // look-ahead stream of the factorization
+    cudaStream_t stream3 = nullptr;           // the gradient, concurrent with assembly + factor
+    cudaEvent_t ev_prep = nullptr, ev_grad = nullptr;
+    // a gradient launched on stream3 and not yet joined (step_impl / finish_gradient)
+    bool grad_pending = false;
+    bool grad_unlaunched = false;
+    double grad_params[3] = {0, 0, 0};  // alpha, beta, eps
+    const double* grad_pos = nullptr;
+    double* grad_dE = nullptr;
+    double* grad_flat = nullptr;
+    const tpe_penalties* grad_pen = nullptr;
     std::vector<cudaEvent_t> fac_events;      // dependency events (no timing)
     std::string err;
     int32_t num_sms = 0;
