@@ -2,15 +2,16 @@
 //
 // Reference: calculateEnergy / gradientAnalytical / kernelDerivs in
 // src/core/tangentPointEnergy.ts:50-392. Ordered disjoint pairs (I, J) are
-// never materialised: each thread owns one edge I, the J edges stream through
-// shared memory in tiles, and disjointness is tested from endpoint indices.
+// never materialised: the J edges stream through shared memory in tiles and
+// disjointness is tested from endpoint indices.
 //
-// Gradient (adjoint) form: the thread that owns I accumulates every
-// contribution that lands on I's endpoints -- from the ordered pair (I, J)
-// (I first: the l_I^(1-a) chain, the d and e_I terms) and from (J, I) (I
-// second: the l_I chain and the d terms). Pair terms are recomputed, nothing
-// of size E^2 is stored, and no atomics are used (deterministic). The two
-// orders share |d|, d_hat and (|d|+eps)^b.
+// The context's energy and gradient use the symmetric tile-pair form: each
+// unordered pair is evaluated once for both orders (I, J) and (J, I), which
+// share |d|, d_hat and (|d|+eps)^b. The adjoint gradient recomputes the pair
+// terms (nothing of size E^2 is stored) and uses no atomics: every
+// contribution lands in a fixed (edge, partner tile) slot and slots are summed
+// in a fixed order (deterministic). energy_kernel, the edge-owner form, serves
+// the allocation-free entry point, whose scratch is sized for it.
 #include <math.h>
 
 #include "tpe_internal.h"
@@ -147,22 +148,118 @@ __global__ void reduce_partials(const double* __restrict__ partial, int32_t npar
     }
 }
 
-// One kernelDerivs evaluation (tangentPointEnergy.ts:165-244) for edge vector e
-// and a distance vector whose norm pieces are shared: returns f, adds the d
-// derivative into dd and the e derivative into de (when DE).
-template <int MODE, bool DE>
-__device__ __forceinline__ double kernel_derivs(double ex, double ey, double ez, double dx,
-                                                double dy, double dz, double hx, double hy,
-                                                double hz, double invDPowB, double invDe,
-                                                double alpha, double beta, double eps,
-                                                double* dd, double* de) {
+// ---- symmetric (tile-pair) forms ---------------------------------------------
+//
+// Each unordered pair {I, J} of edges is evaluated once: the grid covers the
+// tiles (bi, bj), bi <= bj, of 128 x 128 edges; thread t owns I = 128 bi + t and
+// walks the J of tile bj (J > I inside a diagonal tile). Both orders (I, J) and
+// (J, I) share |d|, d_hat and (|d|+eps)^-b per endpoint combination, so the
+// pair work is about half of the edge-owner form. Deterministic: the J-side
+// gradient contributions of a warp's 32 lanes are summed by a fixed shuffle
+// tree, the four warps' sums in a fixed order, and every (edge, partner tile)
+// partial is written exactly once.
+
+// Upper tile (bi <= bj) of the packed index x over a T x T tile grid.
+__device__ __forceinline__ void upper_tile(int x, int& bi, int& bj) {
+    int t = (int)((sqrt(8.0 * (double)x + 1.0) - 1.0) * 0.5);
+    while ((t + 1) * (t + 2) / 2 <= x) t++;
+    while (t * (t + 1) / 2 > x) t--;
+    bj = t;
+    bi = x - t * (t + 1) / 2;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+energy_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
+                  const int2* __restrict__ edges, int32_t E, double alpha, double beta, double eps,
+                  double* __restrict__ partial) {
+    __shared__ double4 sa[kTile], sb[kTile];
+    __shared__ int2 se[kTile];
+    __shared__ double red[kThreads / 32];
+    const int32_t c = blockIdx.z;
+    ea += (int64_t)c * E;
+    eb += (int64_t)c * E;
+    int bi, bj;
+    upper_tile(blockIdx.x, bi, bj);
+    const int32_t I = bi * kTile + threadIdx.x;
+    const bool valid = I < E;
+    double4 a = make_double4(0, 0, 0, 0), b = a;
+    int2 ei = make_int2(-1, -1);
+    if (valid) {
+        a = ea[I];
+        b = eb[I];
+        ei = edges[I];
+    }
+    {
+        const int32_t J = bj * kTile + threadIdx.x;
+        if (J < E) {
+            sa[threadIdx.x] = ea[J];
+            sb[threadIdx.x] = eb[J];
+            se[threadIdx.x] = edges[J];
+        }
+    }
+    __syncthreads();
+    const double eIx = b.x - a.x, eIy = b.y - a.y, eIz = b.z - a.z;
+    const double powI = b.w, ellI = a.w;
+    const int32_t nt = min(kTile, E - bj * kTile);
+    const int32_t js = (bi == bj) ? (int32_t)threadIdx.x + 1 : 0;
+    double acc = 0.0;
+    if (valid) {
+        for (int32_t jj = js; jj < nt; jj++) {
+            if (!disjoint(ei, se[jj])) continue;
+            const double4 qa = sa[jj], qb = sb[jj];
+            const double eJx = qb.x - qa.x, eJy = qb.y - qa.y, eJz = qb.z - qa.z;
+            double sumF = 0.0, sumF2 = 0.0;
+#pragma unroll
+            for (int s2 = 0; s2 < 4; s2++) {
+                const double px = (s2 < 2) ? a.x : b.x, py = (s2 < 2) ? a.y : b.y,
+                             pz = (s2 < 2) ? a.z : b.z;
+                const double qx = (s2 & 1) ? qb.x : qa.x, qy = (s2 & 1) ? qb.y : qa.y,
+                             qz = (s2 & 1) ? qb.z : qa.z;
+                const double dx = px - qx, dy = py - qy, dz = pz - qz;
+                const double invDn = 1.0 / (sqrt(dx * dx + dy * dy + dz * dz) + eps);
+                const double iDb = (MODE == 1) ? pow_b<1>(invDn, beta) : 0.0;
+                const double cx = eIy * dz - eIz * dy, cy = eIz * dx - eIx * dz,
+                             cz = eIx * dy - eIy * dx;
+                const double cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
+                const double kx = eJy * dz - eJz * dy, ky = eJz * dx - eJx * dz,
+                             kz = eJx * dy - eJy * dx;
+                const double kn = sqrt(kx * kx + ky * ky + kz * kz) + eps;
+                if (MODE == 1) {
+                    sumF += pow_a<1>(cn, alpha) * iDb;
+                    sumF2 += pow_a<1>(kn, alpha) * iDb;
+                } else {
+                    const double den = pow(1.0 / invDn, beta);
+                    sumF += pow(cn, alpha) / den;
+                    sumF2 += pow(kn, alpha) / den;
+                }
+            }
+            acc += powI * qa.w * sumF + qb.w * ellI * sumF2;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; w++) t += red[w];
+        partial[(int64_t)c * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// f, d-derivative and e-derivative of one kernelDerivs evaluation
+// (tangentPointEnergy.ts:165-244) as vectors.
+template <int MODE>
+__device__ __forceinline__ double kd_vec(double ex, double ey, double ez, double dx, double dy,
+                                         double dz, double hx, double hy, double hz,
+                                         double invDPowB, double invDe, double alpha, double beta,
+                                         double eps, double (&dd)[3], double (&de)[3]) {
     const double cx = ey * dz - ez * dy;
     const double cy = ez * dx - ex * dz;
     const double cz = ex * dy - ey * dx;
     const double rc = sqrt(cx * cx + cy * cy + cz * cz);
     const double ce = rc + eps;
-    const double cPowA = pow_a<MODE>(ce, alpha);
-    const double f = cPowA * invDPowB;
+    const double f = pow_a<MODE>(ce, alpha) * invDPowB;
     const double coeff_c = alpha * pow_a1<MODE>(ce, alpha) * invDPowB;
     const double coeff_d = -beta * f * invDe;
     double ux = 0, uy = 0, uz = 0, vx = 0, vy = 0, vz = 0;
@@ -171,32 +268,42 @@ __device__ __forceinline__ double kernel_derivs(double ex, double ey, double ez,
         ux = inv * (cy * ez - cz * ey);
         uy = inv * (cz * ex - cx * ez);
         uz = inv * (cx * ey - cy * ex);
-        if (DE) {
-            vx = inv * (dy * cz - dz * cy);
-            vy = inv * (dz * cx - dx * cz);
-            vz = inv * (dx * cy - dy * cx);
-        }
+        vx = inv * (dy * cz - dz * cy);
+        vy = inv * (dz * cx - dx * cz);
+        vz = inv * (dx * cy - dy * cx);
     }
-    dd[0] += coeff_c * ux + coeff_d * hx;
-    dd[1] += coeff_c * uy + coeff_d * hy;
-    dd[2] += coeff_c * uz + coeff_d * hz;
-    if (DE) {
-        de[0] += coeff_c * vx;
-        de[1] += coeff_c * vy;
-        de[2] += coeff_c * vz;
-    }
+    dd[0] = coeff_c * ux + coeff_d * hx;
+    dd[1] = coeff_c * uy + coeff_d * hy;
+    dd[2] = coeff_c * uz + coeff_d * hz;
+    de[0] = coeff_c * vx;
+    de[1] = coeff_c * vy;
+    de[2] = coeff_c * vz;
     return f;
 }
 
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Gradient partials edge_acc[slot][K][6] (endpoint 1 xyz, endpoint 2 xyz) and
+// energy partials: the tile (bi, bj) writes slot bj of its I edges and slot bi
+// of its J edges (both slot bi on a diagonal tile). The gather sums all slots.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads)
-grad_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
-            const int2* __restrict__ edges, int32_t E, int32_t jchunk, double alpha, double beta,
-            double eps, double* __restrict__ edge_acc, double* __restrict__ partial) {
+grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
+                const int2* __restrict__ edges, int32_t E, double alpha, double beta, double eps,
+                double* __restrict__ edge_acc, double* __restrict__ partial) {
     __shared__ double4 sa[kTile], sb[kTile];
+    __shared__ double4 sh[kTile];  // J: unit tangent xyz, (1-a) l^-a
     __shared__ int2 se[kTile];
+    __shared__ double accJ[kThreads / 32][kTile][6];
     __shared__ double red[kThreads / 32];
-    const int32_t I = blockIdx.x * kThreads + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int bi, bj;
+    upper_tile(blockIdx.x, bi, bj);
+    const bool diag = bi == bj;
+    const int32_t I = bi * kTile + threadIdx.x;
     const bool valid = I < E;
     double4 a = make_double4(0, 0, 0, 1), b = make_double4(0, 0, 0, 1);
     int2 ei = make_int2(-1, -1);
@@ -206,45 +313,62 @@ grad_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
         ei = edges[I];
     }
     const double eIx = b.x - a.x, eIy = b.y - a.y, eIz = b.z - a.z;
-    const double reI = sqrt(eIx * eIx + eIy * eIy + eIz * eIz);
     double hIx = 0, hIy = 0, hIz = 0;
-    if (!(reI < 1e-14)) {
-        const double inv = 1.0 / reI;
-        hIx = inv * eIx;
-        hIy = inv * eIy;
-        hIz = inv * eIz;
+    {
+        const double reI = sqrt(eIx * eIx + eIy * eIy + eIz * eIz);
+        if (!(reI < 1e-14)) {
+            const double inv = 1.0 / reI;
+            hIx = inv * eIx;
+            hIy = inv * eIy;
+            hIz = inv * eIz;
+        }
     }
     const double ellI = a.w, powI = b.w;
-    const double dPowCoeff = (1.0 - alpha) * pow(ellI, -alpha);
+    const double dPowI = (1.0 - alpha) * pow(ellI, -alpha);
+    {
+        const int32_t J = bj * kTile + threadIdx.x;
+        double4 qa = make_double4(0, 0, 0, 1), qb = make_double4(0, 0, 0, 1);
+        int2 ej = make_int2(-2, -2);
+        if (J < E) {
+            qa = ea[J];
+            qb = eb[J];
+            ej = edges[J];
+        }
+        sa[threadIdx.x] = qa;
+        sb[threadIdx.x] = qb;
+        se[threadIdx.x] = ej;
+        const double ex = qb.x - qa.x, ey = qb.y - qa.y, ez = qb.z - qa.z;
+        const double re = sqrt(ex * ex + ey * ey + ez * ez);
+        double4 h = make_double4(0, 0, 0, (1.0 - alpha) * pow(qa.w, -alpha));
+        if (!(re < 1e-14)) {
+            const double inv = 1.0 / re;
+            h.x = inv * ex;
+            h.y = inv * ey;
+            h.z = inv * ez;
+        }
+        sh[threadIdx.x] = h;
+    }
+    __syncthreads();
+    const int32_t nt = min(kTile, E - bj * kTile);
     double g1[3] = {0, 0, 0}, g2[3] = {0, 0, 0};
     double en = 0.0;
-    const int32_t j0 = blockIdx.y * jchunk;
-    const int32_t j1 = min(E, j0 + jchunk);
-    for (int32_t t0 = j0; t0 < j1; t0 += kTile) {
-        const int32_t nt = min(kTile, j1 - t0);
-        __syncthreads();
-        if (threadIdx.x < nt) {
-            sa[threadIdx.x] = ea[t0 + threadIdx.x];
-            sb[threadIdx.x] = eb[t0 + threadIdx.x];
-            se[threadIdx.x] = edges[t0 + threadIdx.x];
-        }
-        __syncthreads();
-        if (!valid) continue;
-        for (int32_t jj = 0; jj < nt; jj++) {
-            const int2 ej = se[jj];
-            if (!disjoint(ei, ej)) continue;
-            const double4 qa = sa[jj], qb = sb[jj];
+    for (int32_t jj = 0; jj < nt; jj++) {
+        const int2 ej = se[jj];
+        const bool act = valid && (!diag || jj > (int32_t)threadIdx.x) && disjoint(ei, ej);
+        double cJ[6] = {0, 0, 0, 0, 0, 0};
+        if (act) {
+            const double4 qa = sa[jj], qb = sb[jj], hJ = sh[jj];
             const double eJx = qb.x - qa.x, eJy = qb.y - qa.y, eJz = qb.z - qa.z;
             const double ellJ = qa.w, powJ = qb.w;
             double sumF = 0.0, sumF2 = 0.0;
-            double dd_own[2][3] = {{0, 0, 0}, {0, 0, 0}};  // (I,J): d-derivative at I endpoint a
-            double dd_oth[2][3] = {{0, 0, 0}, {0, 0, 0}};  // (J,I): d-derivative landing on I endpoint a
-            double de[3] = {0, 0, 0};
+            double ownI[2][3] = {{0, 0, 0}, {0, 0, 0}}, othI[2][3] = {{0, 0, 0}, {0, 0, 0}};
+            double ownJ[2][3] = {{0, 0, 0}, {0, 0, 0}}, othJ[2][3] = {{0, 0, 0}, {0, 0, 0}};
+            double deI[3] = {0, 0, 0}, deJ[3] = {0, 0, 0};
 #pragma unroll
-            for (int s = 0; s < 4; s++) {
-                const int ai = s >> 1, bj = s & 1;
+            for (int s2 = 0; s2 < 4; s2++) {
+                const int ai = s2 >> 1, bk = s2 & 1;
                 const double px = ai ? b.x : a.x, py = ai ? b.y : a.y, pz = ai ? b.z : a.z;
-                const double qx = bj ? qb.x : qa.x, qy = bj ? qb.y : qa.y, qz = bj ? qb.z : qa.z;
+                const double qx = bk ? qb.x : qa.x, qy = bk ? qb.y : qa.y, qz = bk ? qb.z : qa.z;
                 const double dx = px - qx, dy = py - qy, dz = pz - qz;  // p_I - p_J
                 const double rd = sqrt(dx * dx + dy * dy + dz * dz);
                 double hx = 0, hy = 0, hz = 0;
@@ -256,46 +380,95 @@ grad_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
                 }
                 const double invDe = 1.0 / (rd + eps);
                 const double invDPowB = (MODE == 1) ? pow_b<1>(invDe, beta) : 1.0 / pow(rd + eps, beta);
-                // (I, J): e = e_I, d = p_I - p_J
-                sumF += kernel_derivs<MODE, true>(eIx, eIy, eIz, dx, dy, dz, hx, hy, hz, invDPowB,
-                                                  invDe, alpha, beta, eps, dd_own[ai], de);
-                // (J, I): e = e_J, d' = p_J - p_I = -d, d_hat' = -d_hat
-                sumF2 += kernel_derivs<MODE, false>(eJx, eJy, eJz, -dx, -dy, -dz, -hx, -hy, -hz,
-                                                    invDPowB, invDe, alpha, beta, eps, dd_oth[ai],
-                                                    nullptr);
+                double ddIJ[3], deIJ[3], ddJI[3], deJI[3];
+                sumF += kd_vec<MODE>(eIx, eIy, eIz, dx, dy, dz, hx, hy, hz, invDPowB, invDe, alpha,
+                                     beta, eps, ddIJ, deIJ);
+                sumF2 += kd_vec<MODE>(eJx, eJy, eJz, -dx, -dy, -dz, -hx, -hy, -hz, invDPowB, invDe,
+                                      alpha, beta, eps, ddJI, deJI);
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    ownI[ai][q] += ddIJ[q];
+                    othI[ai][q] += ddJI[q];
+                    deI[q] += deIJ[q];
+                    ownJ[bk][q] += ddJI[q];
+                    othJ[bk][q] += ddIJ[q];
+                    deJ[q] += deJI[q];
+                }
             }
-            const double base = 0.25 * powI * ellJ;   // (I,J) weight
-            const double base2 = 0.25 * powJ * ellI;  // (J,I) weight
-            const double sI = 0.25 * ellJ * sumF;     // times d(l_I^(1-a))
-            const double sJ2 = 0.25 * powJ * sumF2;   // times d(l_I) for (J,I)
-            en += base * sumF;
-            const double t1 = sI * dPowCoeff;
+            const double baseIJ = 0.25 * powI * ellJ;  // weight of (I, J)
+            const double baseJI = 0.25 * powJ * ellI;  // weight of (J, I)
+            en += baseIJ * sumF + baseJI * sumF2;
+            // I side (the edge-owner form's terms)
+            const double tI = 0.25 * ellJ * sumF * dPowI;
+            const double sI2 = 0.25 * powJ * sumF2;
+            // J side, roles swapped
+            const double tJ = 0.25 * ellI * sumF2 * hJ.w;
+            const double sJ2 = 0.25 * powI * sumF;
+            const double hI[3] = {hIx, hIy, hIz};
+            const double hJv[3] = {hJ.x, hJ.y, hJ.z};
 #pragma unroll
             for (int q = 0; q < 3; q++) {
-                const double h = (q == 0) ? hIx : (q == 1) ? hIy : hIz;
-                g1[q] += -t1 * h + base * dd_own[0][q] - base2 * dd_oth[0][q] - base * de[q] -
-                         sJ2 * h;
-                g2[q] += t1 * h + base * dd_own[1][q] - base2 * dd_oth[1][q] + base * de[q] +
-                         sJ2 * h;
+                g1[q] += -tI * hI[q] + baseIJ * ownI[0][q] - baseJI * othI[0][q] - baseIJ * deI[q] -
+                         sI2 * hI[q];
+                g2[q] += tI * hI[q] + baseIJ * ownI[1][q] - baseJI * othI[1][q] + baseIJ * deI[q] +
+                         sI2 * hI[q];
+                cJ[q] = -tJ * hJv[q] + baseJI * ownJ[0][q] - baseIJ * othJ[0][q] - baseJI * deJ[q] -
+                        sJ2 * hJv[q];
+                cJ[3 + q] = tJ * hJv[q] + baseJI * ownJ[1][q] - baseIJ * othJ[1][q] +
+                            baseJI * deJ[q] + sJ2 * hJv[q];
             }
         }
+        if (__any_sync(0xffffffffu, act)) {
+#pragma unroll
+            for (int q = 0; q < 6; q++) cJ[q] = warp_sum(cJ[q]);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 6; q++) accJ[warp][jj][q] = cJ[q];
+        }
     }
-    if (valid) {
-        double* o = edge_acc + ((int64_t)blockIdx.y * E + I) * 6;
-        o[0] = g1[0];
-        o[1] = g1[1];
-        o[2] = g1[2];
-        o[3] = g2[0];
-        o[4] = g2[1];
-        o[5] = g2[2];
+    __syncthreads();
+    // J side of this tile (fixed warp order), and on a diagonal tile the I side
+    // of the same edge added to it
+    {
+        const int32_t J = bj * kTile + threadIdx.x;
+        if (J < E) {
+            double v[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                double t = 0.0;
+                if ((int32_t)threadIdx.x < nt)
+                    for (int w = 0; w < kThreads / 32; w++) t += accJ[w][threadIdx.x][q];
+                v[q] = t;
+            }
+            if (diag) {
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    v[q] += g1[q];
+                    v[3 + q] += g2[q];
+                }
+            }
+            double* o = edge_acc + ((int64_t)bi * E + J) * 6;
+#pragma unroll
+            for (int q = 0; q < 6; q++) o[q] = v[q];
+        }
+        if (!diag && valid) {
+            double* o = edge_acc + ((int64_t)bj * E + I) * 6;
+            o[0] = g1[0];
+            o[1] = g1[1];
+            o[2] = g1[2];
+            o[3] = g2[0];
+            o[4] = g2[1];
+            o[5] = g2[2];
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) en += __shfl_down_sync(0xffffffffu, en, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = en;
+    en = warp_sum(en);
+    if (lane == 0) red[warp] = en;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < kThreads / 32; w++) s += red[w];
-        partial[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; w++) t += red[w];
+        partial[blockIdx.x] = t;
     }
 }
 
@@ -323,13 +496,6 @@ __global__ void gather_vertex_grad(const double* __restrict__ edge_acc, int32_t 
 
 inline int exp_mode(double alpha, double beta) { return (alpha == 3.0 && beta == 6.0) ? 1 : 0; }
 
-// Number of J chunks so that the grid has roughly 4 blocks per SM.
-inline int32_t pick_chunks(const tpe_ctx* ctx, int32_t E, int32_t ncurves) {
-    const int32_t xb = (E + kThreads - 1) / kThreads;
-    int32_t want = (4 * ctx->num_sms + xb * ncurves - 1) / (xb * ncurves);
-    want = max(1, min(want, (E + kTile - 1) / kTile));
-    return want;
-}
 
 }  // namespace
 
@@ -368,25 +534,22 @@ int32_t edge_prep(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps
 int32_t energy_fp64(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, double eps,
                     double* d_energy) {
     const int32_t E = ctx->E;
-    const int32_t xb = (E + kThreads - 1) / kThreads;
-    const int32_t ny = pick_chunks(ctx, E, ncurves);
-    const int32_t jchunk = ((E + ny - 1) / ny + kTile - 1) / kTile * kTile;
-    const int32_t nyy = (E + jchunk - 1) / jchunk;
-    const int32_t nparts = xb * nyy;
-    TPE_TRY(ensure(ctx, ctx->partial, sizeof(double) * (size_t)nparts * ncurves));
-    dim3 grid(xb, nyy, ncurves);
+    const int32_t T = (E + kTile - 1) / kTile;
+    const int32_t ntiles = T * (T + 1) / 2;
+    TPE_TRY(ensure(ctx, ctx->partial, sizeof(double) * (size_t)ntiles * ncurves));
+    dim3 grid(ntiles, 1, ncurves);
     KernelScope ks(ctx, TPE_KGROUP_ENERGY, 2);
     if (exp_mode(alpha, beta) == 1)
-        energy_kernel<1><<<grid, kThreads, 0, ctx->stream>>>(
+        energy_sym_kernel<1><<<grid, kThreads, 0, ctx->stream>>>(
             ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
-            jchunk, alpha, beta, eps, ctx->partial.as<double>());
+            alpha, beta, eps, ctx->partial.as<double>());
     else
-        energy_kernel<0><<<grid, kThreads, 0, ctx->stream>>>(
+        energy_sym_kernel<0><<<grid, kThreads, 0, ctx->stream>>>(
             ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
-            jchunk, alpha, beta, eps, ctx->partial.as<double>());
+            alpha, beta, eps, ctx->partial.as<double>());
     TPE_CUDA_TRY(cudaGetLastError());
-    // total = sum(0.25 * l_I^(1-a) * l_J * sumK) / 2
-    reduce_partials<<<ncurves, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), nparts, 0.125,
+    // total = sum over ordered pairs of 0.25 * l^(1-a) * l * sumK, halved
+    reduce_partials<<<ncurves, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), ntiles, 0.125,
                                                       d_energy);
     TPE_CUDA_TRY(cudaGetLastError());
     return TPE_OK;
@@ -422,31 +585,29 @@ int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
                          double* d_grad) {
     const int32_t E = ctx->E, V = ctx->V;
-    const int32_t xb = (E + kThreads - 1) / kThreads;
-    const int32_t ny = pick_chunks(ctx, E, 1);
-    const int32_t jchunk = ((E + ny - 1) / ny + kTile - 1) / kTile * kTile;
-    const int32_t nyy = (E + jchunk - 1) / jchunk;
-    TPE_TRY(ensure(ctx, ctx->edge_acc, sizeof(double) * 6 * (size_t)E * nyy));
-    TPE_TRY(ensure(ctx, ctx->partial, sizeof(double) * (size_t)xb * nyy));
-    dim3 grid(xb, nyy, 1);
+    const int32_t T = (E + kTile - 1) / kTile;
+    const int32_t ntiles = T * (T + 1) / 2;
+    TPE_TRY(ensure(ctx, ctx->edge_acc, sizeof(double) * 6 * (size_t)E * T));
+    TPE_TRY(ensure(ctx, ctx->partial, sizeof(double) * (size_t)ntiles));
     KernelScope ks(ctx, TPE_KGROUP_GRADIENT, 1 + (d_grad ? 1 : 0) + (d_energy ? 1 : 0));
     if (exp_mode(alpha, beta) == 1)
-        grad_kernel<1><<<grid, kThreads, 0, ctx->stream>>>(
-            ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
-            jchunk, alpha, beta, eps, ctx->edge_acc.as<double>(), ctx->partial.as<double>());
+        grad_sym_kernel<1><<<ntiles, kThreads, 0, ctx->stream>>>(
+            ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E, alpha,
+            beta, eps, ctx->edge_acc.as<double>(), ctx->partial.as<double>());
     else
-        grad_kernel<0><<<grid, kThreads, 0, ctx->stream>>>(
-            ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E,
-            jchunk, alpha, beta, eps, ctx->edge_acc.as<double>(), ctx->partial.as<double>());
+        grad_sym_kernel<0><<<ntiles, kThreads, 0, ctx->stream>>>(
+            ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E, alpha,
+            beta, eps, ctx->edge_acc.as<double>(), ctx->partial.as<double>());
     TPE_CUDA_TRY(cudaGetLastError());
     if (d_grad) {
         gather_vertex_grad<<<(V + 127) / 128, 128, 0, ctx->stream>>>(
-            ctx->edge_acc.as<double>(), nyy, E, ctx->d_inc_off.as<int32_t>(),
+            ctx->edge_acc.as<double>(), T, E, ctx->d_inc_off.as<int32_t>(),
             ctx->d_inc.as<int32_t>(), V, d_grad);
         TPE_CUDA_TRY(cudaGetLastError());
     }
     if (d_energy) {
-        reduce_partials<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), xb * nyy, 0.5,
+        // the partials already carry the 1/4 weight: halve for the ordered-pair sum
+        reduce_partials<<<1, 256, 0, ctx->stream>>>(ctx->partial.as<double>(), ntiles, 0.5,
                                                     d_energy);
         TPE_CUDA_TRY(cudaGetLastError());
     }
