@@ -84,6 +84,15 @@ __global__ void split_copy_kernel(const float* __restrict__ S, int32_t ld, int32
 constexpr int kPw = 32;        // panel width inside a diagonal block
 constexpr int kPl = kPw + 1;   // row stride of the panel scratch
 
+// Decodes the packed lower-triangular index e into (ti, tj), tj <= ti.
+__device__ __forceinline__ void tri_decode(int e, int& ti, int& tj) {
+    int t = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+    while ((t + 1) * (t + 2) / 2 <= e) t++;
+    while (t * (t + 1) / 2 > e) t--;
+    ti = t;
+    tj = e - t * (t + 1) / 2;
+}
+
 // Column K of the in-register Cholesky of a 32 x 32 block (lane = row):
 // pivot from lane K, scale column K, update the columns right of it; the
 // template recursion keeps every register index static.
@@ -112,75 +121,116 @@ __device__ __forceinline__ void chol_col(float (&v)[32], int lane, bool& brk, fl
     }
 }
 
-// Decodes the packed lower-triangular index e into (ti, tj), tj <= ti.
-__device__ __forceinline__ void tri_decode(int e, int& ti, int& tj) {
-    int t = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
-    while ((t + 1) * (t + 2) / 2 <= e) t++;
-    while (t * (t + 1) / 2 > e) t--;
-    ti = t;
-    tj = e - t * (t + 1) / 2;
+// Warp-level factor of the 32 x 32 diagonal part of panel c0 (lane = row,
+// column values shared by shuffles, no block barriers), then its inverse by
+// forward substitution (lane = column of the inverse) into z, 1/L_ii into rd.
+// Not inlined: the unrolled body is long, and a single copy shared by the
+// four panels is fetched into the instruction cache once per launch instead of
+// once per call site.
+__device__ __noinline__ void warp_factor32(float* a, float* z, float* rd, int c0, int lane,
+                                              int32_t* bad) {
+    float v[kPw];
+#pragma unroll
+    for (int m = 0; m < kPw; m++) v[m] = (m <= lane) ? a[(c0 + lane) * kLd + c0 + m] : 0.0f;
+    bool brk = false;
+    float myrs = 1.0f;
+    chol_col<0>(v, lane, brk, myrs);
+    if (brk && lane == 0) atomicExch(bad, 1);
+#pragma unroll
+    for (int m = 0; m < kPw; m++) a[(c0 + lane) * kLd + c0 + m] = (m <= lane) ? v[m] : 0.0f;
+    rd[c0 + lane] = myrs;
+    __syncwarp();
+    float x[kPw];
+#pragma unroll
+    for (int i = 0; i < kPw; i++) x[i] = (i == lane) ? 1.0f : 0.0f;
+#pragma unroll
+    for (int k = 0; k < kPw; k++) {
+        x[k] *= rd[c0 + k];
+#pragma unroll
+        for (int i = k + 1; i < kPw; i++) x[i] -= a[(c0 + i) * kLd + c0 + k] * x[k];
+    }
+#pragma unroll
+    for (int i = 0; i < kPw; i++) z[(c0 + i) * kLd + c0 + lane] = (i >= lane) ? x[i] : 0.0f;
+    __syncwarp();
 }
 
-// One CTA factors the 128 x 128 diagonal block at (j0, j0) of S (lower
-// triangle read) and writes L_jj (split, zero above the diagonal) to L,
-// Z_jj = L_jj^{-1} (split, lower) to Z and W_jj = Z_jj^T (split, upper) to W.
+// a[R..R+3][C..C+3] -= pl[4ti..][.] pl[4tj..][.]^T over the 32 panel columns.
+__device__ __forceinline__ void update_tile(float* a, const float* pl, int ti, int tj, int base) {
+    float acc[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+#pragma unroll 4
+    for (int k = 0; k < kPw; k++) {
+        float pr[4], pc[4];
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+            pr[x] = pl[(4 * ti + x) * kPl + k];
+            pc[x] = pl[(4 * tj + x) * kPl + k];
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) acc[x][y] += pr[x] * pc[y];
+    }
+    const int R = base + 4 * ti, Cc = base + 4 * tj;
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) a[(R + x) * kLd + Cc + y] -= acc[x][y];
+}
+
+// One CTA factors the 128 x 128 diagonal block at (j0, j0) of S (its lower
+// triangle) and writes Z_jj = L_jj^{-1} (split, zero above the diagonal) to Z.
+// L_jj itself is not needed outside (the panel solve uses Z_jj, the inverse
+// uses only the blocks below the diagonal), and W_jj = Z_jj^T is written by
+// diag_transpose_kernel once the whole factorization is done.
 //
-// Blocked right-looking over four 32-column panels. Warp 0 factors a panel's
-// 32 x 32 diagonal part in registers (lane = row, column values shared by
-// shuffles, no block barriers) and inverts it by forward substitution (lane =
-// column of the inverse). All eight warps then solve the rows below against
-// that inverse (warp = 4 columns, lane = row) and apply the rank-32 update to
-// the lower trailing triangle in 4 x 4 register tiles. The off-diagonal
+// Blocked right-looking over four 32-column panels with an in-CTA look-ahead:
+// warp 0 factors a panel's 32 x 32 diagonal part in registers and inverts it
+// (warp_factor32); all eight warps solve the rows below against that inverse
+// (warp = 4 columns, lane = row); then warp 0 alone applies the rank-32 update
+// to the next panel's diagonal part and factors it, while warps 1-7 update
+// the rest of the trailing triangle (4 x 4 register tiles). The off-diagonal
 // 32 x 32 blocks of the inverse follow from Z_ab = -Z_aa sum_{b<=c<a} L_ac Z_cb,
-// one block distance at a time, in the same 4 x 4 tiling. Reciprocal square
-// roots are the fast approximate ones: the factor is a preconditioner, CG
-// restores FP64 accuracy. *bad = 1 when a pivot is not positive and finite.
+// one block distance at a time. Reciprocal square roots are the fast
+// approximate ones: the factor is a preconditioner, CG restores FP64 accuracy.
+// *bad = 1 when a pivot is not positive and finite.
 __global__ void __launch_bounds__(256, 2)
-potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __restrict__ Lhi,
-                float* __restrict__ Llo, float* __restrict__ Zhi, float* __restrict__ Zlo,
-                float* __restrict__ Whi, float* __restrict__ Wlo, int32_t* __restrict__ bad) {
+potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __restrict__ Zhi,
+                float* __restrict__ Zlo, int32_t* __restrict__ bad) {
     extern __shared__ float sm[];
-    float* a = sm;                  // the block, then L (lower)
+    float* a = sm;                  // the block, then L (lower; the upper part is never read)
     float* z = a + kT * kLd;        // L^{-1} (lower)
     float* pl = z + kT * kLd;       // 96 x 33 panel rows / block products
     float* rd = pl + 96 * kPl;      // 1 / L_ii
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < kT * kT; e += 256) {
-        const int r = e >> 7, c = e & (kT - 1);
-        a[r * kLd + c] = (c <= r) ? S[(size_t)(j0 + r) * ld + j0 + c] : 0.0f;
-        z[r * kLd + c] = 0.0f;
+    {
+        // whole block, 16-byte loads (ld and j0 are multiples of 128)
+        float4 buf[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int e = tid + 256 * q;  // float4 index
+            const int r = e >> 5, c = (e & 31) * 4;
+            buf[q] = *reinterpret_cast<const float4*>(S + (size_t)(j0 + r) * ld + j0 + c);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const int e = tid + 256 * q;
+            const int r = e >> 5, c = (e & 31) * 4;
+            a[r * kLd + c] = buf[q].x;
+            a[r * kLd + c + 1] = buf[q].y;
+            a[r * kLd + c + 2] = buf[q].z;
+            a[r * kLd + c + 3] = buf[q].w;
+        }
     }
     __syncthreads();
-    for (int p = 0; p < kT / kPw; p++) {
+    if (warp == 0) warp_factor32(a, z, rd, 0, lane, bad);
+    __syncthreads();
+    for (int p = 0; p < kT / kPw - 1; p++) {
         const int c0 = p * kPw;
-        if (warp == 0) {
-            float v[kPw];
-#pragma unroll
-            for (int m = 0; m < kPw; m++) v[m] = (m <= lane) ? a[(c0 + lane) * kLd + c0 + m] : 0.0f;
-            bool brk = false;
-            float myrs = 1.0f;
-            chol_col<0>(v, lane, brk, myrs);
-            if (brk && lane == 0) atomicExch(bad, 1);
-#pragma unroll
-            for (int m = 0; m < kPw; m++) a[(c0 + lane) * kLd + c0 + m] = (m <= lane) ? v[m] : 0.0f;
-            rd[c0 + lane] = myrs;
-            __syncwarp();
-            // column `lane` of the inverse: forward substitution, axpy form
-            float x[kPw];
-#pragma unroll
-            for (int i = 0; i < kPw; i++) x[i] = (i == lane) ? 1.0f : 0.0f;
-#pragma unroll
-            for (int k = 0; k < kPw; k++) {
-                x[k] *= rd[c0 + k];
-#pragma unroll
-                for (int i = k + 1; i < kPw; i++) x[i] -= a[(c0 + i) * kLd + c0 + k] * x[k];
-            }
-#pragma unroll
-            for (int i = 0; i < kPw; i++) z[(c0 + i) * kLd + c0 + lane] = (i >= lane) ? x[i] : 0.0f;
-        }
-        __syncthreads();
         const int nr = kT - c0 - kPw;
-        if (nr == 0) break;
         // panel rows below: pl[r][m] = sum_k A[c0+32+r][c0+k] * Zd[m][k]
         {
             const int m0 = 4 * warp;
@@ -199,42 +249,29 @@ potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __re
             }
         }
         __syncthreads();
-        // rank-32 update of the lower trailing triangle, 4 x 4 tiles
-        {
-            const int nt = nr / 4;
-            const int ntiles = nt * (nt + 1) / 2;
-            for (int e = tid; e < ntiles; e += 256) {
+        const int base = c0 + kPw;
+        const int nt = nr / 4;
+        const int ntiles = nt * (nt + 1) / 2;
+        constexpr int kNext = 36;  // 4 x 4 tiles of the next 32 x 32 diagonal part (packed first)
+        if (warp == 0) {
+            for (int e = lane; e < kNext; e += 32) {
                 int ti, tj;
                 tri_decode(e, ti, tj);
-                float acc[4][4];
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
-#pragma unroll 4
-                for (int k = 0; k < kPw; k++) {
-                    float pr[4], pc[4];
-#pragma unroll
-                    for (int x = 0; x < 4; x++) {
-                        pr[x] = pl[(4 * ti + x) * kPl + k];
-                        pc[x] = pl[(4 * tj + x) * kPl + k];
-                    }
-#pragma unroll
-                    for (int x = 0; x < 4; x++)
-#pragma unroll
-                        for (int y = 0; y < 4; y++) acc[x][y] += pr[x] * pc[y];
-                }
-                const int R = c0 + kPw + 4 * ti, Cc = c0 + kPw + 4 * tj;
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) a[(R + x) * kLd + Cc + y] -= acc[x][y];
+                update_tile(a, pl, ti, tj, base);
             }
-        }
-        // the panel rows become final L
-        for (int e = tid; e < nr * kPw; e += 256) {
-            const int r = e >> 5, m = e & 31;
-            a[(c0 + kPw + r) * kLd + c0 + m] = pl[r * kPl + m];
+            __syncwarp();
+            warp_factor32(a, z, rd, base, lane, bad);
+        } else {
+            for (int e = kNext + tid - 32; e < ntiles; e += 224) {
+                int ti, tj;
+                tri_decode(e, ti, tj);
+                update_tile(a, pl, ti, tj, base);
+            }
+            // the panel rows become final L
+            for (int e = tid - 32; e < nr * kPw; e += 224) {
+                const int r = e >> 5, m = e & 31;
+                a[(base + r) * kLd + c0 + m] = pl[r * kPl + m];
+            }
         }
         __syncthreads();
     }
@@ -300,20 +337,33 @@ potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __re
         }
         __syncthreads();
     }
-    // stores: lane = column (coalesced rows, conflict-free shared reads)
+    // Z_jj (split): lane = column, coalesced rows
     for (int e = tid; e < kT * kT; e += 256) {
         const int r = e >> 7, c = e & (kT - 1);
         const size_t o = (size_t)(j0 + r) * ld + j0 + c;
         float h, l;
-        split32(c <= r ? a[r * kLd + c] : 0.0f, h, l);
-        Lhi[o] = h;
-        Llo[o] = l;
         split32(c <= r ? z[r * kLd + c] : 0.0f, h, l);
         Zhi[o] = h;
         Zlo[o] = l;
-        split32(r <= c ? z[c * kLd + r] : 0.0f, h, l);
-        Whi[o] = h;
-        Wlo[o] = l;
+    }
+}
+
+// W_jj = Z_jj^T for every diagonal block (blockIdx.z = block), split.
+__global__ void diag_transpose_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
+                                      float* __restrict__ whi, float* __restrict__ wlo, int32_t ld) {
+    __shared__ float th[32][33], tl[32][33];
+    const int32_t j0 = blockIdx.z * kT;
+    const int32_t r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const size_t o = (size_t)(j0 + r0 + yy) * ld + j0 + c0 + threadIdx.x;
+        th[yy][threadIdx.x] = zhi[o];
+        tl[yy][threadIdx.x] = zlo[o];
+    }
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const size_t o = (size_t)(j0 + c0 + yy) * ld + j0 + r0 + threadIdx.x;
+        whi[o] = th[threadIdx.x][yy];
+        wlo[o] = tl[threadIdx.x][yy];
     }
 }
 
@@ -657,8 +707,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
         int last_rest = -1;
         for (int j = 0; j < nb; j++) {
             const int32_t j0 = j * kT;
-            potrf128_kernel<<<1, 256, potrf_smem, st>>>(S, Vp, j0, mf.L.hi, mf.L.lo, mf.Z.hi,
-                                                        mf.Z.lo, mf.W.hi, mf.W.lo, d_bad);
+            potrf128_kernel<<<1, 256, potrf_smem, st>>>(S, Vp, j0, mf.Z.hi, mf.Z.lo, d_bad);
             TPE_CUDA_TRY(cudaGetLastError());
             if (j + 1 == nb) break;
             const int32_t rows = Vp - j0 - kT;
@@ -709,6 +758,12 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, v, d_err, st));
         }
         if (last_rest >= 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[last_rest], 0));
+    }
+    {
+        KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
+        diag_transpose_kernel<<<dim3(kT / 32, kT / 32, nb), dim3(32, 8), 0, st>>>(
+            mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp);
+        TPE_CUDA_TRY(cudaGetLastError());
     }
     {
         // Z = L^{-1} level by level (W = Z^T alongside)
