@@ -337,7 +337,7 @@ int32_t launch_gradient(tpe_ctx* ctx) {
     {
         StreamSwap sw(ctx, ctx->stream3);
         TPE_TRY(energy_grad_fp64(ctx, ctx->grad_params[0], ctx->grad_params[1], ctx->grad_params[2],
-                                 nullptr, ctx->grad_dE));
+                                 nullptr, ctx->grad_dE, ctx->grad_sms));
     }
     TPE_CUDA_TRY(cudaEventRecord(ctx->ev_grad, ctx->stream3));
     return TPE_OK;
@@ -1137,6 +1137,11 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
         return nullptr;
     }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    ctx->grad_sms = ctx->num_sms / 3;
+    if (const char* g = getenv("TPE_GRAD_SMS")) {
+        const int n = atoi(g);
+        if (n >= 0) ctx->grad_sms = n;  // 0: an ordinary grid over all SMs
+    }
     if (status) *status = TPE_OK;
     return ctx;
 }
@@ -1157,7 +1162,7 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
                       &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,
                       &ctx->mx_Wlo, &ctx->mx_Thi, &ctx->mx_Tlo, &ctx->mx_vec, &ctx->mx_part,
-                      &ctx->mx_Zd, &ctx->mx_Wd};
+                      &ctx->mx_Zd, &ctx->mx_Wd, &ctx->grad_ctr, &ctx->mx_ctr};
     for (DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     for (auto& p : ctx->prof_pending) {

@@ -23,6 +23,8 @@
 // whenever the FP32 factorization breaks down or CG does not converge.
 #include <math.h>
 
+#include <algorithm>
+
 #include "tc.h"
 #include "tpe_internal.h"
 
@@ -667,6 +669,10 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
     int32_t* d_bad = ctx->status.as<int32_t>() + 2;
     TPE_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 2 * sizeof(int32_t), st));
+    // tile counters of the persistent trailing updates, one per panel
+    TPE_TRY(ensure(ctx, ctx->mx_ctr, sizeof(int32_t) * (size_t)(Vp / kT)));
+    int32_t* d_ctr = ctx->mx_ctr.as<int32_t>();
+    TPE_CUDA_TRY(cudaMemsetAsync(d_ctr, 0, sizeof(int32_t) * (size_t)(Vp / kT), st));
     int32_t* d_err = d_bad + 1;
     double* d = ctx->mx_d.as<double>();
     float* S = ctx->mx_S.as<float>();
@@ -698,6 +704,10 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     cudaEvent_t* ev_t = ctx->fac_events.data();        // trsm of panel j done
     cudaEvent_t* ev_r = ctx->fac_events.data() + nb;   // rest of panel j done
     const cudaStream_t st2 = ctx->stream2;
+    // The trailing updates run persistent (one CTA per SM walking its tiles) on
+    // the SMs left by the concurrent gradient, minus a few kept free so that the
+    // chain's potrf / trsm / strip launches never wait for a whole update.
+    const int32_t rest_ctas = std::max(16, ctx->num_sms - ctx->grad_sms - 8);
     {
         const int64_t nrest = nb > 2 ? nb - 2 : 0;
         KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + 3 * (int64_t)(nb - 1) + nrest);
@@ -738,7 +748,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
                 u.mode = tc::kLowerTiles;
                 u.alpha = -1.0f;
                 u.beta = 1.0f;
-                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2));
+                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2, rest_ctas, d_ctr + j));
                 TPE_CUDA_TRY(cudaEventRecord(ev_r[j], st2));
             }
             if (last_rest >= 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[last_rest], 0));

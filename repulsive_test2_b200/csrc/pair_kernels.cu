@@ -14,6 +14,8 @@
 // the allocation-free entry point, whose scratch is sized for it.
 #include <math.h>
 
+#include <algorithm>
+
 #include "tpe_internal.h"
 
 namespace tpe {
@@ -286,24 +288,44 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Shared memory of one 128-thread tile worker.
+struct GradSmem {
+    double4 sa[kTile], sb[kTile];
+    double4 sh[kTile];  // J: unit tangent xyz, (1-a) l^-a
+    int2 se[kTile];
+    double accJ[kThreads / 32][kTile][6];
+    double red[kThreads / 32];
+};
+
+// Barrier over the 128 threads of one tile worker (named barrier bar; 0 is the
+// whole-block barrier of a 128-thread block).
+__device__ __forceinline__ void worker_sync(int bar) {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(kThreads) : "memory");
+}
+
 // Gradient partials edge_acc[slot][K][6] (endpoint 1 xyz, endpoint 2 xyz) and
-// energy partials: the tile (bi, bj) writes slot bj of its I edges and slot bi
-// of its J edges (both slot bi on a diagonal tile). The gather sums all slots.
+// energy partials of upper tile x: the tile (bi, bj) writes slot bj of its I
+// edges and slot bi of its J edges (both slot bi on a diagonal tile). The
+// gather sums all slots. tid < 128 is the thread's index in its worker.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads)
-grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
-                const int2* __restrict__ edges, int32_t E, double alpha, double beta, double eps,
-                double* __restrict__ edge_acc, double* __restrict__ partial) {
-    __shared__ double4 sa[kTile], sb[kTile];
-    __shared__ double4 sh[kTile];  // J: unit tangent xyz, (1-a) l^-a
-    __shared__ int2 se[kTile];
-    __shared__ double accJ[kThreads / 32][kTile][6];
-    __shared__ double red[kThreads / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ __forceinline__ void grad_sym_tile(int x, int tid, int bar, GradSmem& sm,
+                                              const double4* __restrict__ ea,
+                                              const double4* __restrict__ eb,
+                                              const int2* __restrict__ edges, int32_t E,
+                                              double alpha, double beta, double eps,
+                                              double* __restrict__ edge_acc,
+                                              double* __restrict__ partial) {
+    double4* sa = sm.sa;
+    double4* sb = sm.sb;
+    double4* sh = sm.sh;
+    int2* se = sm.se;
+    double(*accJ)[kTile][6] = sm.accJ;
+    double* red = sm.red;
+    const int lane = tid & 31, warp = tid >> 5;
     int bi, bj;
-    upper_tile(blockIdx.x, bi, bj);
+    upper_tile(x, bi, bj);
     const bool diag = bi == bj;
-    const int32_t I = bi * kTile + threadIdx.x;
+    const int32_t I = bi * kTile + tid;
     const bool valid = I < E;
     double4 a = make_double4(0, 0, 0, 1), b = make_double4(0, 0, 0, 1);
     int2 ei = make_int2(-1, -1);
@@ -326,7 +348,7 @@ grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
     const double ellI = a.w, powI = b.w;
     const double dPowI = (1.0 - alpha) * pow(ellI, -alpha);
     {
-        const int32_t J = bj * kTile + threadIdx.x;
+        const int32_t J = bj * kTile + tid;
         double4 qa = make_double4(0, 0, 0, 1), qb = make_double4(0, 0, 0, 1);
         int2 ej = make_int2(-2, -2);
         if (J < E) {
@@ -334,9 +356,9 @@ grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
             qb = eb[J];
             ej = edges[J];
         }
-        sa[threadIdx.x] = qa;
-        sb[threadIdx.x] = qb;
-        se[threadIdx.x] = ej;
+        sa[tid] = qa;
+        sb[tid] = qb;
+        se[tid] = ej;
         const double ex = qb.x - qa.x, ey = qb.y - qa.y, ez = qb.z - qa.z;
         const double re = sqrt(ex * ex + ey * ey + ez * ez);
         double4 h = make_double4(0, 0, 0, (1.0 - alpha) * pow(qa.w, -alpha));
@@ -346,15 +368,15 @@ grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
             h.y = inv * ey;
             h.z = inv * ez;
         }
-        sh[threadIdx.x] = h;
+        sh[tid] = h;
     }
-    __syncthreads();
+    worker_sync(bar);
     const int32_t nt = min(kTile, E - bj * kTile);
     double g1[3] = {0, 0, 0}, g2[3] = {0, 0, 0};
     double en = 0.0;
     for (int32_t jj = 0; jj < nt; jj++) {
         const int2 ej = se[jj];
-        const bool act = valid && (!diag || jj > (int32_t)threadIdx.x) && disjoint(ei, ej);
+        const bool act = valid && (!diag || jj > (int32_t)tid) && disjoint(ei, ej);
         double cJ[6] = {0, 0, 0, 0, 0, 0};
         if (act) {
             const double4 qa = sa[jj], qb = sb[jj], hJ = sh[jj];
@@ -427,18 +449,18 @@ grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
             for (int q = 0; q < 6; q++) accJ[warp][jj][q] = cJ[q];
         }
     }
-    __syncthreads();
+    worker_sync(bar);
     // J side of this tile (fixed warp order), and on a diagonal tile the I side
     // of the same edge added to it
     {
-        const int32_t J = bj * kTile + threadIdx.x;
+        const int32_t J = bj * kTile + tid;
         if (J < E) {
             double v[6];
 #pragma unroll
             for (int q = 0; q < 6; q++) {
                 double t = 0.0;
-                if ((int32_t)threadIdx.x < nt)
-                    for (int w = 0; w < kThreads / 32; w++) t += accJ[w][threadIdx.x][q];
+                if ((int32_t)tid < nt)
+                    for (int w = 0; w < kThreads / 32; w++) t += accJ[w][tid][q];
                 v[q] = t;
             }
             if (diag) {
@@ -464,11 +486,50 @@ grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
     }
     en = warp_sum(en);
     if (lane == 0) red[warp] = en;
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    worker_sync(bar);
+    if (tid == 0) {
         double t = 0.0;
         for (int w = 0; w < kThreads / 32; w++) t += red[w];
-        partial[blockIdx.x] = t;
+        partial[x] = t;
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+grad_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
+                const int2* __restrict__ edges, int32_t E, double alpha, double beta, double eps,
+                double* __restrict__ edge_acc, double* __restrict__ partial) {
+    __shared__ GradSmem sm;
+    grad_sym_tile<MODE>(blockIdx.x, threadIdx.x, 0, sm, ea, eb, edges, E, alpha, beta, eps,
+                        edge_acc, partial);
+}
+
+// The same tiles on a bounded number of SMs: kGradWorkers independent 128-thread
+// workers per block (one block per SM: the registers of three workers fill it)
+// take tiles from a global counter until all ntiles are done. Every tile writes
+// its own partial slots, so the result does not depend on which worker took it.
+// Used for the gradient that runs beside the factorization, which then keeps
+// the remaining SMs for its latency-bound chain.
+constexpr int kGradWorkers = 3;
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads * kGradWorkers, 1)
+grad_sym_persist_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
+                        const int2* __restrict__ edges, int32_t E, double alpha, double beta,
+                        double eps, double* __restrict__ edge_acc, double* __restrict__ partial,
+                        int32_t ntiles, int32_t* __restrict__ counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int w = threadIdx.x / kThreads, tid = threadIdx.x % kThreads;
+    GradSmem& sm = reinterpret_cast<GradSmem*>(smem_raw)[w];
+    __shared__ int next[kGradWorkers];
+    for (;;) {
+        if (tid == 0) next[w] = atomicAdd(counter, 1);
+        worker_sync(1 + w);
+        const int x = next[w];
+        worker_sync(1 + w);
+        if (x >= ntiles) break;
+        grad_sym_tile<MODE>(x, tid, 1 + w, sm, ea, eb, edges, E, alpha, beta, eps, edge_acc,
+                            partial);
     }
 }
 
@@ -583,21 +644,34 @@ int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2
 }
 
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
-                         double* d_grad) {
+                         double* d_grad, int32_t max_blocks) {
     const int32_t E = ctx->E, V = ctx->V;
     const int32_t T = (E + kTile - 1) / kTile;
     const int32_t ntiles = T * (T + 1) / 2;
     TPE_TRY(ensure(ctx, ctx->edge_acc, sizeof(double) * 6 * (size_t)E * T));
     TPE_TRY(ensure(ctx, ctx->partial, sizeof(double) * (size_t)ntiles));
     KernelScope ks(ctx, TPE_KGROUP_GRADIENT, 1 + (d_grad ? 1 : 0) + (d_energy ? 1 : 0));
-    if (exp_mode(alpha, beta) == 1)
+    const int mode = exp_mode(alpha, beta);
+    if (max_blocks > 0) {
+        TPE_TRY(ensure(ctx, ctx->grad_ctr, sizeof(int32_t)));
+        TPE_CUDA_TRY(cudaMemsetAsync(ctx->grad_ctr.ptr, 0, sizeof(int32_t), ctx->stream));
+        const size_t smem = sizeof(GradSmem) * kGradWorkers;
+        const unsigned nb = (unsigned)std::min<int64_t>(max_blocks, (ntiles + kGradWorkers - 1) / kGradWorkers);
+        auto kern = mode == 1 ? grad_sym_persist_kernel<1> : grad_sym_persist_kernel<0>;
+        TPE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<nb, kThreads * kGradWorkers, smem, ctx->stream>>>(
+            ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E, alpha,
+            beta, eps, ctx->edge_acc.as<double>(), ctx->partial.as<double>(), ntiles,
+            ctx->grad_ctr.as<int32_t>());
+    } else if (mode == 1) {
         grad_sym_kernel<1><<<ntiles, kThreads, 0, ctx->stream>>>(
             ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E, alpha,
             beta, eps, ctx->edge_acc.as<double>(), ctx->partial.as<double>());
-    else
+    } else {
         grad_sym_kernel<0><<<ntiles, kThreads, 0, ctx->stream>>>(
             ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), E, alpha,
             beta, eps, ctx->edge_acc.as<double>(), ctx->partial.as<double>());
+    }
     TPE_CUDA_TRY(cudaGetLastError());
     if (d_grad) {
         gather_vertex_grad<<<(V + 127) / 128, 128, 0, ctx->stream>>>(

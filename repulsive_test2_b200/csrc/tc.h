@@ -54,8 +54,13 @@ struct GemmArgs {
     float alpha = 1.0f, beta = 0.0f;
 };
 
+// max_ctas > 0 selects the persistent form (at most max_ctas CTAs, one per SM,
+// each walking many tiles) for whole-tile TMA epilogues; tile_ctr (device, may be
+// null) is then a zeroed counter the CTAs take tiles from, else tiles go
+// round-robin.
 cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const GemmArgs& g,
-                    int32_t* err, cudaStream_t stream);
+                    int32_t* err, cudaStream_t stream, int32_t max_ctas = 0,
+                    int32_t* tile_ctr = nullptr);
 
 }  // namespace tc
 }  // namespace tpe

@@ -11,6 +11,7 @@
 // copies it issued land, frees its tensor memory and returns.
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "tc.h"
@@ -407,6 +408,299 @@ gemm_nt_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__
                      : "memory");
 }
 
+// ---- persistent form ----------------------------------------------------------
+//
+// The same product with one CTA per SM walking many output tiles: warp 0 is
+// the TMA producer, warp 1 issues the MMAs into one of two TMEM accumulators
+// (256 columns), warps 2-5 drain the other accumulator through a 32 KB staging
+// buffer and TMA stores / reduce-adds, so a tile's epilogue overlaps the next
+// tile's loads and MMAs and the set-up (barriers, TMEM, tensor maps) is paid
+// once per SM. Tiles come from a device counter (zeroed by the caller) when one
+// is given, else round-robin. The tile index travels from the producer to the
+// MMA thread in the ring slot of the tile's first stage and from there to the
+// epilogue with the accumulator, each published by an ordinary mbarrier
+// arrive (release) before the consumer's wait (acquire). TMA epilogues only
+// (whole 128 x 128 tiles).
+constexpr int kPThreads = 192;
+constexpr int kOutBytes = 2 * kTileBytes;  // epilogue staging: 2 x (128 rows x 32 columns)
+constexpr int kPSmemBytes = kStages * kStageBytes + kOutBytes + 1024 + 256;
+static_assert(kPSmemBytes <= 232448, "persistent GEMM shared memory exceeds the per-block limit");
+
+__device__ __forceinline__ void decode_tile(int x, const GemmArgs& g, int tm, int tn, int& z,
+                                            int& ti, int& tj) {
+    const int per = (g.mode & kLowerTiles) ? tm * (tm + 1) / 2 : tm * tn;
+    z = x / per;
+    const int r = x - z * per;
+    if (g.mode & kLowerTiles) {
+        int t = (int)((sqrtf(8.0f * (float)r + 1.0f) - 1.0f) * 0.5f);
+        while ((t + 1) * (t + 2) / 2 <= r) t++;
+        while (t * (t + 1) / 2 > r) t--;
+        ti = t;
+        tj = r - t * (t + 1) / 2;
+    } else {
+        ti = r / tn;
+        tj = r - ti * tn;
+    }
+}
+
+__device__ __forceinline__ void tile_k_range(const GemmArgs& g, int ti, int& k_begin, int& nk) {
+    int kb = 0, ke = g.K;
+    if (g.mode & kAUpper) kb = min(g.K, ti * kBM);
+    if (g.mode & kALower) ke = min(g.K, (ti + 1) * kBM);
+    k_begin = kb;
+    nk = ke > kb ? (ke - kb) / kBK : 0;
+}
+
+__device__ __forceinline__ void epi_sync() {
+    asm volatile("bar.sync 1, 128;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kPThreads, 1)
+gemm_nt_persist_kernel(const __grid_constant__ CUtensorMap a_hi,
+                       const __grid_constant__ CUtensorMap a_lo,
+                       const __grid_constant__ CUtensorMap b_hi,
+                       const __grid_constant__ CUtensorMap b_lo,
+                       const __grid_constant__ CUtensorMap c_hi,
+                       const __grid_constant__ CUtensorMap c_lo, const KParams P, int32_t tm,
+                       int32_t tn, int32_t ntiles, int32_t* __restrict__ tile_ctr) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* stage_out = smem + kStages * kStageBytes;
+    // full[S], empty[S], acc_full[2], acc_empty[2], done
+    uint64_t* bars = (uint64_t*)(stage_out + kOutBytes);
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * kStages + 5);
+    volatile int32_t* aborted = (volatile int32_t*)(tmem_slot + 1);
+    volatile int32_t* tileq = aborted + 1;          // [kStages]
+    volatile int32_t* accq = tileq + kStages;       // [2]
+    const GemmArgs& g = P.g;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages),
+                   accf0 = smem_u32(bars + 2 * kStages), acce0 = smem_u32(bars + 2 * kStages + 2),
+                   done = smem_u32(bars + 2 * kStages + 4);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(accf0 + 8 * b, 2);    // the MMA thread's arrive + the MMA commit
+            mbar_init(acce0 + 8 * b, 128);  // every epilogue thread
+        }
+        mbar_init(done, 1);
+        *aborted = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(2 * kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int it = 0;  // ring slots used so far
+            for (int i = 0;; i++) {
+                int x = tile_ctr ? atomicAdd(tile_ctr, 1) : (int)blockIdx.x + i * (int)gridDim.x;
+                if (x >= ntiles) x = -1;
+                int z = 0, ti = 0, tj = 0, kb = 0, nk = 0;
+                if (x >= 0) {
+                    decode_tile(x, g, tm, tn, z, ti, tj);
+                    tile_k_range(g, ti, kb, nk);
+                }
+                const int32_t ax = g.a_c0 + z * g.a_zc + kb, ay = g.a_r0 + z * g.a_zr + ti * kBM;
+                const int32_t bx = g.b_c0 + z * g.b_zc + kb, by = g.b_r0 + z * g.b_zr + tj * kBN;
+                const int nslots = nk > 0 ? nk : 1;
+                bool stop = false;
+                for (int k = 0; k < nslots; k++, it++) {
+                    const int s = it % kStages;
+                    if (it >= kStages &&
+                        !mbar_wait(empty0 + 8 * s, ((it / kStages) - 1) & 1, P.err)) {
+                        *aborted = 1;
+                        stop = true;
+                        break;
+                    }
+                    if (*aborted) {
+                        stop = true;
+                        break;
+                    }
+                    const uint32_t fb = full0 + 8 * s;
+                    if (k == 0) tileq[s] = x;
+                    if (nk == 0) {
+                        mbar_arrive(fb);  // the index alone (end of work or an empty K range)
+                        continue;
+                    }
+                    const uint32_t st = smem_u32(smem + s * kStageBytes);
+                    mbar_expect_tx(fb, kStageBytes);
+                    const int32_t kk = k * kBK;
+                    tma_load_2d(st, &a_hi, fb, ax + kk, ay);
+                    tma_load_2d(st + kTileBytes, &a_lo, fb, ax + kk, ay);
+                    tma_load_2d(st + 2 * kTileBytes, &b_hi, fb, bx + kk, by);
+                    tma_load_2d(st + 3 * kTileBytes, &b_lo, fb, bx + kk, by);
+                }
+                if (stop || x < 0) break;
+            }
+            // every copy issued has landed before the CTA may exit
+            for (int j = it > kStages ? it - kStages : 0; j < it; j++)
+                mbar_wait(full0 + 8 * (j % kStages), (j / kStages) & 1, P.err);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int it = 0;
+            bool any = false;
+            for (int i = 0;; i++) {
+                const int b = i & 1;
+                int s = it % kStages;
+                if (!mbar_wait(full0 + 8 * s, (it / kStages) & 1, P.err)) {
+                    *aborted = 1;
+                    break;
+                }
+                const int x = tileq[s];
+                if (i >= 2 && !mbar_wait(acce0 + 8 * b, ((i >> 1) - 1) & 1, P.err)) {
+                    *aborted = 1;
+                    break;
+                }
+                accq[b] = x;
+                mbar_arrive(accf0 + 8 * b);  // publishes accq[b]
+                int z = 0, ti = 0, tj = 0, kb = 0, nk = 0;
+                if (x >= 0) {
+                    decode_tile(x, g, tm, tn, z, ti, tj);
+                    tile_k_range(g, ti, kb, nk);
+                }
+                if (nk == 0) {
+                    mbar_arrive(empty0 + 8 * s);
+                    mbar_arrive(accf0 + 8 * b);
+                    it++;
+                    if (x < 0) break;
+                    continue;
+                }
+                const uint32_t d = tmem + (uint32_t)(b * kTmemCols);
+                bool stop = false;
+                for (int k = 0; k < nk; k++, it++) {
+                    s = it % kStages;
+                    if (k > 0 && !mbar_wait(full0 + 8 * s, (it / kStages) & 1, P.err)) {
+                        *aborted = 1;
+                        stop = true;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t st = smem_u32(smem + s * kStageBytes);
+#pragma unroll
+                    for (int kk = 0; kk < kBK / 8; kk++) {
+                        const uint64_t ah = sw128_desc(st + kk * 32);
+                        const uint64_t al = sw128_desc(st + kTileBytes + kk * 32);
+                        const uint64_t bh = sw128_desc(st + 2 * kTileBytes + kk * 32);
+                        const uint64_t bl = sw128_desc(st + 3 * kTileBytes + kk * 32);
+                        mma_tf32(d, ah, bh, (k | kk) ? 1u : 0u);
+                        mma_tf32(d, ah, bl, 1u);
+                        mma_tf32(d, al, bh, 1u);
+                    }
+                    mma_commit(empty0 + 8 * s);
+                    any = true;
+                }
+                if (stop) break;
+                mma_commit(accf0 + 8 * b);
+            }
+            if (any)
+                mma_commit(done);
+            else
+                mbar_arrive(done);
+        }
+        __syncwarp();
+    } else {
+        // epilogue: warps 2-5 own TMEM lane quarters (warp % 4)
+        const int q4 = warp & 3;
+        const int r = q4 * 32 + lane;
+        const bool issuer = threadIdx.x == 64;
+        const bool split_out = P.c_lo != nullptr;
+        const float alpha = g.alpha;
+        int cc = 0;  // staging chunks used so far
+        for (int i = 0;; i++) {
+            const int b = i & 1;
+            if (!mbar_wait(accf0 + 8 * b, (i >> 1) & 1, P.err)) {
+                *aborted = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int x = accq[b];
+            if (x < 0) break;
+            int z, ti, tj, kb, nk;
+            decode_tile(x, g, tm, tn, z, ti, tj);
+            tile_k_range(g, ti, kb, nk);
+            const int32_t x0 = g.c_c0 + z * g.c_zc + tj * kBN, y0 = g.c_r0 + z * g.c_zr + ti * kBM;
+            for (int c = 0; c < 4; c++, cc++) {
+                float v[32];
+                if (nk > 0) {
+                    tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(b * kTmemCols + 32 * c),
+                              v);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 32; e++) v[e] = 0.0f;
+                }
+                if (c == 3) {
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    mbar_arrive(acce0 + 8 * b);
+                }
+                uint8_t* buf = stage_out + (split_out ? 0 : (cc & 1) * kTileBytes);
+                if (issuer) {
+                    if (split_out)
+                        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                    else
+                        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                }
+                epi_sync();
+                uint8_t* row_hi = buf + r * 128;
+                uint8_t* row_lo = buf + kTileBytes + r * 128;
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int pq = (q ^ (r & 7)) * 16;
+                    float4 y = make_float4(alpha * v[4 * q], alpha * v[4 * q + 1],
+                                           alpha * v[4 * q + 2], alpha * v[4 * q + 3]);
+                    if (split_out) {
+                        float4 h, l;
+                        split(y.x, h.x, l.x);
+                        split(y.y, h.y, l.y);
+                        split(y.z, h.z, l.z);
+                        split(y.w, h.w, l.w);
+                        *reinterpret_cast<float4*>(row_hi + pq) = h;
+                        *reinterpret_cast<float4*>(row_lo + pq) = l;
+                    } else {
+                        *reinterpret_cast<float4*>(row_hi + pq) = y;
+                    }
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                epi_sync();
+                if (issuer) {
+                    const uint32_t src = smem_u32(buf);
+                    if (P.tma_epi == 2)
+                        tma_reduce_add_2d(&c_hi, src, x0 + 32 * c, y0);
+                    else
+                        tma_store_2d(&c_hi, src, x0 + 32 * c, y0);
+                    if (split_out) tma_store_2d(&c_lo, smem_u32(buf + kTileBytes), x0 + 32 * c, y0);
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
+            }
+            if (*aborted) break;
+        }
+        if (issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        mbar_wait(done, 0, P.err);  // every MMA issued has completed
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(2 * kTmemCols)
+                     : "memory");
+    }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -447,7 +741,7 @@ bool make_maps(SplitMat& m) {
 }
 
 cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const GemmArgs& g,
-                    int32_t* err, cudaStream_t stream) {
+                    int32_t* err, cudaStream_t stream, int32_t max_ctas, int32_t* tile_ctr) {
     if (g.M <= 0 || g.N <= 0 || g.nbatch <= 0) return cudaSuccess;
     // TMA x coordinates must be multiples of 4 FP32 elements (16 bytes); whole
     // K stages only (callers pad to 128).
@@ -485,6 +779,17 @@ cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const Gem
             P.tma_epi = 1;
         else if (g.beta == 1.0f && !C.lo)
             P.tma_epi = 2;
+    }
+    const int64_t ntiles = (int64_t)grid.x * grid.y * grid.z;
+    if (max_ctas > 0 && P.tma_epi != 0 && ntiles > 1 && ntiles < (1LL << 30)) {
+        e = cudaFuncSetAttribute(gemm_nt_persist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kPSmemBytes);
+        if (e != cudaSuccess) return e;
+        const unsigned nb = (unsigned)std::min<int64_t>(ntiles, max_ctas);
+        gemm_nt_persist_kernel<<<nb, kPThreads, kPSmemBytes, stream>>>(
+            A.map_hi, A.map_lo, B.map_hi, B.map_lo, C.map_hi, C.map_lo, P, tm, tn, (int32_t)ntiles,
+            tile_ctr);
+        return cudaGetLastError();
     }
     gemm_nt_kernel<<<grid, 128, kSmemBytes, stream>>>(A.map_hi, A.map_lo, B.map_hi, B.map_lo,
                                                       C.map_hi, C.map_lo, P);

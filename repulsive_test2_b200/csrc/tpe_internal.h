@@ -107,6 +107,9 @@ struct tpe_ctx {
     double* grad_dE = nullptr;
     double* grad_flat = nullptr;
     const tpe_penalties* grad_pen = nullptr;
+    // SMs the concurrent gradient may occupy; the rest stay free for the
+    // factorization's chain of small launches (TPE_GRAD_SMS overrides)
+    int32_t grad_sms = 0;
     std::vector<cudaEvent_t> fac_events;      // dependency events (no timing)
     std::string err;
     int32_t num_sms = 0;
@@ -122,6 +125,8 @@ struct tpe_ctx {
     // per-evaluation buffers
     tpe::DevBuf pos, pos2, pos3, edge_a, edge_b, grad, edge_acc, partial, scalars, flat0, flat1,
         flat2, flat3, dir;
+    tpe::DevBuf grad_ctr;  // tile counter of the SM-bounded gradient kernel
+    tpe::DevBuf mx_ctr;    // tile counters of the persistent trailing updates
     tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
     tpe::DevBuf edge_m;                     // mixed-precision edge records (4 float4 per edge)
     tpe::DevBuf mat_A, mat_L, mat_Linv, mat_B, mat_B0;
@@ -177,9 +182,10 @@ int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2
                             int32_t V, int32_t E, double alpha, double beta, double eps,
                             double4* ea, double4* eb, double* partial, int32_t max_parts,
                             double* d_energy);
-// Energy (optional) and gradient (interleaved V x 3) of one curve.
+// Energy (optional) and gradient (interleaved V x 3) of one curve. max_blocks > 0
+// bounds the SMs the pair kernel occupies (one block per SM).
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
-                         double* d_grad);
+                         double* d_grad, int32_t max_blocks = 0);
 
 // ---- mixed precision pair kernels (pair_mixed.cu) ----------------------------
 int32_t edge_prep_mixed(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps,
