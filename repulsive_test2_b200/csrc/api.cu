@@ -317,6 +317,8 @@ int32_t check_topology(tpe_ctx* ctx) {
     return TPE_OK;
 }
 
+}  // namespace
+
 // ---- gradient on the side stream ---------------------------------------------
 
 // Launches issued while in scope go to stream s (KernelScope events included).
@@ -355,6 +357,8 @@ int32_t finish_gradient(tpe_ctx* ctx) {
     return interleaved_to_block(ctx, ctx->grad_dE, ctx->grad_flat, ctx->V);
 }
 
+namespace {
+
 // ---- saddle operator ----------------------------------------------------------
 
 // Factor A_rho and the Schur complement from ctx->mat_A (V x V) and ctx->con_C (k x 3V).
@@ -374,6 +378,8 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
     op.C = ctx->con_C.as<double>();
     op.W = nullptr;
     op.w_src = nullptr;
+    op.large = false;
+    op.Ainv = op.Sinv = nullptr;
     *singular = false;
     const int32_t nb = (V + kNB - 1) / kNB;
     TPE_TRY(ensure(ctx, ctx->mat_L, sizeof(double) * (size_t)V * V));
@@ -458,29 +464,43 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
             *singular = true;
             return TPE_OK;
         }
-        TPE_TRY(load_rhs());
-        for (int32_t r0 = 0; r0 < nrhs; r0 += 64) {
-            const int32_t nr = (nrhs - r0) < 64 ? (nrhs - r0) : 64;
-            TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, op.Y + (size_t)r0 * V, nr));
+        if (k > kLargeSchur) {
+            // explicit inverses, Y by gathers, the Schur complement on the device
+            op.large = true;
+            op.Scc.clear();
+            bool sing = false;
+            TPE_TRY(large_schur_build(ctx, op, b_flat, &sing));
+            if (sing) {
+                *singular = true;
+                return TPE_OK;
+            }
+        } else {
+            TPE_TRY(load_rhs());
+            for (int32_t r0 = 0; r0 < nrhs; r0 += 64) {
+                const int32_t nr = (nrhs - r0) < 64 ? (nrhs - r0) : 64;
+                TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, op.Y + (size_t)r0 * V, nr));
+            }
         }
     }
     if (k > 0) {
-        TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * ((size_t)k * k + 4 * (size_t)k + 16)));
+        TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * ((op.large ? 0 : (size_t)k * k) +
+                                                         4 * (size_t)k + 16)));
         double* dS = ctx->tmp.as<double>();
-        TPE_TRY(gram_dots(ctx, op.C, k, op.Y, k, 3 * (int64_t)V, dS));
-        double* dR = dS + (size_t)k * k;
+        if (!op.large) TPE_TRY(gram_dots(ctx, op.C, k, op.Y, k, 3 * (int64_t)V, dS));
+        double* dR = dS + (op.large ? 0 : (size_t)k * k);
         { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
         row_stats_kernel<<<k, 256, 0, ctx->stream>>>(op.C, V, dR); }
         TPE_CUDA_TRY(cudaGetLastError());
         std::vector<double> rs((size_t)4 * k);
-        TPE_TRY(download(ctx, op.Scc.data(), dS, sizeof(double) * (size_t)k * k));
+        if (!op.large) TPE_TRY(download(ctx, op.Scc.data(), dS, sizeof(double) * (size_t)k * k));
         TPE_TRY(download(ctx, rs.data(), dR, sizeof(double) * 4 * (size_t)k));
         // symmetrise the Gram matrix (two sides of one dot product)
-        for (int32_t i = 0; i < k; i++)
-            for (int32_t j = i + 1; j < k; j++) {
-                const double a = 0.5 * (op.Scc[(size_t)i * k + j] + op.Scc[(size_t)j * k + i]);
-                op.Scc[(size_t)i * k + j] = op.Scc[(size_t)j * k + i] = a;
-            }
+        if (!op.large)
+            for (int32_t i = 0; i < k; i++)
+                for (int32_t j = i + 1; j < k; j++) {
+                    const double a = 0.5 * (op.Scc[(size_t)i * k + j] + op.Scc[(size_t)j * k + i]);
+                    op.Scc[(size_t)i * k + j] = op.Scc[(size_t)j * k + i] = a;
+                }
         const double su = 1.0 / sqrt((double)V);
         double cu_abs = 0.0, c_abs = 0.0;
         for (int32_t r = 0; r < k; r++) {
@@ -494,7 +514,7 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
             *singular = true;
             return TPE_OK;
         }
-        if (!host_chol(op.Scc, k)) {
+        if (!op.large && !host_chol(op.Scc, k)) {
             *singular = true;
             return TPE_OK;
         }
@@ -503,9 +523,18 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
             // M = Scu^T Scc^{-1} Scu (3 x 3 SPD)
             op.M.assign(9, 0.0);
             std::vector<std::vector<double>> Z(3, std::vector<double>((size_t)k));
-            for (int c = 0; c < 3; c++) {
-                for (int32_t r = 0; r < k; r++) Z[c][r] = op.Scu[(size_t)r * 3 + c];
-                host_chol_solve(op.Scc, k, Z[c]);
+            if (op.large) {
+                std::vector<double> su3((size_t)3 * k), z3((size_t)3 * k);
+                for (int c = 0; c < 3; c++)
+                    for (int32_t r = 0; r < k; r++) su3[(size_t)c * k + r] = op.Scu[(size_t)r * 3 + c];
+                TPE_TRY(large_schur_apply(ctx, op, su3.data(), 3, z3.data()));
+                for (int c = 0; c < 3; c++)
+                    Z[c].assign(z3.begin() + (size_t)c * k, z3.begin() + (size_t)(c + 1) * k);
+            } else {
+                for (int c = 0; c < 3; c++) {
+                    for (int32_t r = 0; r < k; r++) Z[c][r] = op.Scu[(size_t)r * 3 + c];
+                    host_chol_solve(op.Scc, k, Z[c]);
+                }
             }
             for (int a = 0; a < 3; a++)
                 for (int b = 0; b < 3; b++) {
@@ -553,14 +582,22 @@ int32_t op_build(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int32_t k, 
 
 // Multipliers of the bordered Schur system for the reduced right-hand side
 // rc = C w - d (k) and ru = U^T w (3): lam (k) and mu (3).
-void schur_multipliers(const SaddleOp& op, const std::vector<double>& rc, const double* ru,
-                       std::vector<double>& lam, double mu[3]) {
+int32_t schur_multipliers(tpe_ctx* ctx, const SaddleOp& op, const std::vector<double>& rc,
+                          const double* ru, std::vector<double>& lam, double mu[3]) {
     const int32_t k = op.k;
     lam.assign((size_t)k, 0.0);
     mu[0] = mu[1] = mu[2] = 0.0;
-    if (k == 0) return;
+    if (k == 0) return TPE_OK;
+    auto scc_solve = [&](std::vector<double>& b) -> int32_t {
+        if (op.large) {
+            std::vector<double> in = b;
+            return large_schur_apply(ctx, op, in.data(), 1, b.data());
+        }
+        host_chol_solve(op.Scc, k, b);
+        return TPE_OK;
+    };
     std::vector<double> t = rc;
-    host_chol_solve(op.Scc, k, t);
+    TPE_TRY(scc_solve(t));
     if (op.trans_constrained) {
         std::vector<double> rhs(3);
         for (int c = 0; c < 3; c++) {
@@ -573,17 +610,18 @@ void schur_multipliers(const SaddleOp& op, const std::vector<double>& rc, const 
         std::vector<double> r2 = rc;
         for (int32_t r = 0; r < k; r++)
             for (int c = 0; c < 3; c++) r2[r] -= op.Scu[(size_t)r * 3 + c] * mu[c];
-        host_chol_solve(op.Scc, k, r2);
+        TPE_TRY(scc_solve(r2));
         lam = r2;
     } else {
         lam = t;
     }
+    return TPE_OK;
 }
 
-// Solve with the current operator: b_flat (device, 3V, or null = 0), d (host, k,
-// or null = 0). x_flat (device) and lam (host) out. residual computed when non-null.
-int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_flat,
-                 std::vector<double>& lam, double* residual) {
+// One solve with the current operator: b_flat (device, 3V, or null = 0), d
+// (host, k, or null = 0). x_flat (device) and lam (host) out.
+int32_t op_solve_once(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_flat,
+                      std::vector<double>& lam) {
     SaddleOp& op = ctx->op;
     const int32_t V = op.V, k = op.k;
     const int64_t m = 3 * (int64_t)V;
@@ -606,6 +644,8 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
                               "mixed-precision solve did not converge");
                     return TPE_ERR_REFINE_NOT_CONVERGED;
                 }
+            } else if (op.large) {
+                TPE_TRY(mrhs_fp64(ctx, op.Ainv, V, b_flat, V, 3, w));
             } else {
                 TPE_TRY(chol_solve_fp64(ctx, op.L, op.Linv, V, w, 3));
             }
@@ -627,9 +667,36 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
     if (d)
         for (int32_t r = 0; r < k; r++) rc[r] -= d[r];
     double mu[3] = {0, 0, 0};
-    schur_multipliers(op, rc, ru.data(), lam, mu);
+    TPE_TRY(schur_multipliers(ctx, op, rc, ru.data(), lam, mu));
     TPE_TRY(combine_solution(ctx, b_flat ? w : nullptr, op.Y, k, lam.data(), mu, op.rho, V,
                              x_flat));
+    return TPE_OK;
+}
+
+// op_solve_once, and with a large constraint set (explicit inverses, accurate
+// to about cond(A_rho) eps) one step of iterative refinement on the FP64
+// residual; residual computed when non-null.
+int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_flat,
+                 std::vector<double>& lam, double* residual) {
+    SaddleOp& op = ctx->op;
+    const int32_t V = op.V, k = op.k;
+    const int64_t m = 3 * (int64_t)V;
+    TPE_TRY(op_solve_once(ctx, b_flat, d, x_flat, lam));
+    if (op.large && b_flat && k > 0) {
+        TPE_TRY(ensure(ctx, ctx->ref_r, sizeof(double) * (size_t)m));
+        TPE_TRY(ensure(ctx, ctx->ref_x, sizeof(double) * (size_t)m));
+        double* rt = ctx->ref_r.as<double>();
+        double* dx = ctx->ref_x.as<double>();
+        std::vector<double> bottom((size_t)k, 0.0), rb((size_t)k, 0.0), dlam;
+        if (d)
+            for (int32_t r = 0; r < k; r++) bottom[r] = d[r];
+        double r0 = 0.0;
+        TPE_TRY(saddle_residual(ctx, op.A, V, op.C, k, x_flat, lam.data(), b_flat, bottom.data(),
+                                &r0, rt, rb.data()));
+        TPE_TRY(op_solve_once(ctx, rt, rb.data(), dx, dlam));
+        TPE_TRY(axpby(ctx, m, 1.0, dx, 1.0, x_flat));
+        for (int32_t r = 0; r < k; r++) lam[r] += dlam[r];
+    }
     if (residual) {
         const double* top = b_flat;
         if (!top) {
@@ -870,7 +937,7 @@ int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, c
             std::vector<double> rc((size_t)k);
             for (int32_t r = 0; r < k; r++) rc[r] = 0.0 - (-ph[r]);
             double mu[3];
-            schur_multipliers(op, rc, ru, lam, mu);
+            TPE_TRY(schur_multipliers(ctx, op, rc, ru, lam, mu));
             const double su = 1.0 / (op.rho * sqrt((double)V));
             for (int32_t r = 0; r < k; r++) coef.push_back(lam[r]);
             for (int c = 0; c < 3; c++) coef.push_back(mu[c] * su);
@@ -1162,7 +1229,10 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
                       &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,
                       &ctx->mx_Wlo, &ctx->mx_Thi, &ctx->mx_Tlo, &ctx->mx_vec, &ctx->mx_part,
-                      &ctx->mx_Zd, &ctx->mx_Wd, &ctx->grad_ctr, &ctx->mx_ctr};
+                      &ctx->mx_Zd, &ctx->mx_Wd, &ctx->grad_ctr, &ctx->mx_ctr, &ctx->mat_Ainv,
+                      &ctx->inv_X, &ctx->inv_W, &ctx->inv_T, &ctx->sch_nz, &ctx->sch_S,
+                      &ctx->sch_L, &ctx->sch_Linv, &ctx->sch_Sinv, &ctx->sch_vec,
+                      &ctx->ref_r, &ctx->ref_x};
     for (DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     for (auto& p : ctx->prof_pending) {

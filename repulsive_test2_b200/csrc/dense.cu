@@ -199,6 +199,18 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
+// Two doubles into 16-byte aligned shared memory from a source that may be
+// only 8-byte aligned (an odd row length).
+template <bool kAligned16>
+__device__ __forceinline__ void cp_async_pair(void* smem, const double* gmem) {
+    if (kAligned16) {
+        cp_async16(smem, gmem);
+    } else {
+        const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s + 8), "l"(gmem + 1));
+    }
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -211,6 +223,7 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
+template <bool kAligned16>  // rows start on 16-byte boundaries (n even)
 __global__ void __launch_bounds__(256)
 gemm_lower_update_kernel(double* __restrict__ L, int32_t n, int32_t r_s, int32_t c_s, int32_t c_e,
                          int32_t k0, int32_t kl) {
@@ -227,8 +240,10 @@ gemm_lower_update_kernel(double* __restrict__ L, int32_t n, int32_t r_s, int32_t
         for (int idx = tid; idx < GT * (GK / 2); idx += 256) {
             const int rr = idx / (GK / 2), pc = (idx % (GK / 2)) * 2;
             const int32_t ra = min(r0 + rr, n - 1), rb = min(c0 + rr, n - 1);
-            cp_async16(As + (size_t)buf * GT * GP + rr * GP + pc, L + (int64_t)ra * n + k0 + kc + pc);
-            cp_async16(Bs + (size_t)buf * GT * GP + rr * GP + pc, L + (int64_t)rb * n + k0 + kc + pc);
+            cp_async_pair<kAligned16>(As + (size_t)buf * GT * GP + rr * GP + pc,
+                                      L + (int64_t)ra * n + k0 + kc + pc);
+            cp_async_pair<kAligned16>(Bs + (size_t)buf * GT * GP + rr * GP + pc,
+                                      L + (int64_t)rb * n + k0 + kc + pc);
         }
         cp_async_commit();
     };
@@ -275,6 +290,143 @@ gemm_lower_update_kernel(double* __restrict__ L, int32_t n, int32_t r_s, int32_t
             if (col < c_e && col <= row) rp[col] -= acc[i][j][0];
             if (col + 1 < c_e && col + 1 <= row) rp[col + 1] -= acc[i][j][1];
         }
+    }
+}
+
+// C = alpha A B^T + beta C (row-major FP64) with the tile, fragment and staging
+// scheme of gemm_lower_update_kernel, separate operands, rows past M / N
+// clamped (never stored), a zero-filled K tail and optional structure:
+// kDLowerTiles computes only tiles with tile column <= tile row; kDAUpper
+// (A[i][k] = 0 for k < i) starts the K loop of tile row t at 128 t, kDALower
+// (A[i][k] = 0 for k > i) ends it at 128 (t + 1).
+template <bool kAligned16>
+__global__ void __launch_bounds__(256) dgemm_nt_kernel(const DGemmArgs g) {
+    extern __shared__ double dsm[];
+    const int32_t ti = blockIdx.y, tj = blockIdx.x;
+    if ((g.mode & kDLowerTiles) && tj > ti) return;
+    const int32_t r0 = ti * GT, c0 = tj * GT;
+    int32_t kb = 0, ke = g.K;
+    if (g.mode & kDAUpper) kb = min(g.K, r0);
+    if (g.mode & kDALower) ke = min(g.K, r0 + GT);
+    double* As = dsm;                // [2][GT][GP]
+    double* Bs = dsm + 2 * GT * GP;  // [2][GT][GP]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = (warp >> 2) * 64, wc = (warp & 3) * 32;
+    const int fr = lane >> 2, fk = lane & 3;
+    auto load = [&](int buf, int kc) {
+        for (int idx = tid; idx < GT * (GK / 2); idx += 256) {
+            const int rr = idx / (GK / 2), pc = (idx % (GK / 2)) * 2;
+            const int32_t k = kb + kc + pc;
+            const int64_t ra = min(r0 + rr, g.M - 1), rb = min(c0 + rr, g.N - 1);
+            double* da = As + (size_t)buf * GT * GP + rr * GP + pc;
+            double* db = Bs + (size_t)buf * GT * GP + rr * GP + pc;
+            if (k + 1 < ke) {
+                cp_async_pair<kAligned16>(da, g.A + ra * g.lda + k);
+                cp_async_pair<kAligned16>(db, g.B + rb * g.ldb + k);
+            } else {
+                da[0] = k < ke ? g.A[ra * g.lda + k] : 0.0;
+                db[0] = k < ke ? g.B[rb * g.ldb + k] : 0.0;
+                da[1] = 0.0;
+                db[1] = 0.0;
+            }
+        }
+        cp_async_commit();
+    };
+    double acc[8][4][2];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    const int nch = ke > kb ? (ke - kb + GK - 1) / GK : 0;
+    if (nch > 0) load(0, 0);
+    for (int ch = 0; ch < nch; ch++) {
+        if (ch + 1 < nch) {
+            load((ch + 1) & 1, (ch + 1) * GK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double* Ab = As + (size_t)(ch & 1) * GT * GP + (wr + fr) * GP + fk;
+        const double* Bb = Bs + (size_t)(ch & 1) * GT * GP + (wc + fr) * GP + fk;
+#pragma unroll
+        for (int kk = 0; kk < GK; kk += 4) {
+            double af[8], bf[4];
+#pragma unroll
+            for (int i = 0; i < 8; i++) af[i] = Ab[i * 8 * GP + kk];
+#pragma unroll
+            for (int j = 0; j < 4; j++) bf[j] = Bb[j * 8 * GP + kk];
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int32_t row = r0 + wr + 8 * i + fr;
+        if (row >= g.M) continue;
+        double* cp = g.C + (int64_t)row * g.ldc;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int32_t col = c0 + wc + 8 * j + 2 * fk;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                if (col + e >= g.N) continue;
+                double y = g.alpha * acc[i][j][e];
+                if (g.beta != 0.0) y += g.beta * cp[col + e];
+                cp[col + e] = y;
+            }
+        }
+    }
+}
+
+// The 64 x 64 diagonal-block inverses (nb x 64 x 64, lower) onto the diagonals
+// of X (lower) and W = X^T (upper), n x n; block b covers min(64, n - 64 b) rows.
+__global__ void diag_inverse_kernel(const double* __restrict__ Linv, int32_t n,
+                                    double* __restrict__ X, double* __restrict__ W) {
+    const int32_t b = blockIdx.x, r0 = b * NB, s = min(NB, n - r0);
+    const double* Li = Linv + (int64_t)b * NB * NB;
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+        const int i = idx / NB, j = idx % NB;
+        if (i >= s || j >= s) continue;
+        X[(int64_t)(r0 + i) * n + r0 + j] = Li[idx];
+        W[(int64_t)(r0 + j) * n + r0 + i] = Li[idx];
+    }
+}
+
+// dst[j][i] = src[i][j] for an m x c block (row strides lds, ldd), 32 x 32 tiles.
+__global__ void transpose_fp64_kernel(const double* __restrict__ src, int64_t lds, int32_t m,
+                                      int32_t c, double* __restrict__ dst, int64_t ldd) {
+    __shared__ double t[32][33];
+    const int32_t i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int32_t i = i0 + r, j = j0 + threadIdx.x;
+        if (i < m && j < c) t[r][threadIdx.x] = src[(int64_t)i * lds + j];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int32_t j = j0 + r, i = i0 + threadIdx.x;
+        if (i < m && j < c) dst[(int64_t)j * ldd + i] = t[threadIdx.x][r];
+    }
+}
+
+// M[i][j] = M[j][i] for j > i (the lower triangle mirrored onto the upper),
+// one 32 x 32 tile pair per block.
+__global__ void mirror_lower_kernel(double* __restrict__ M, int32_t n) {
+    __shared__ double t[32][33];
+    const int32_t bi = blockIdx.y, bj = blockIdx.x;  // source tile (bi, bj), bi >= bj
+    if (bj > bi) return;
+    const int32_t i0 = bi * 32, j0 = bj * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int32_t i = i0 + r, j = j0 + threadIdx.x;
+        if (i < n && j < n) t[r][threadIdx.x] = M[(int64_t)i * n + j];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int32_t row = j0 + r, col = i0 + threadIdx.x;  // (row, col) = (j, i)
+        if (row < n && col < n && col > row) M[(int64_t)row * n + col] = t[threadIdx.x][r];
     }
 }
 
@@ -511,12 +663,13 @@ __global__ void combine_kernel(const double* __restrict__ w, const double* __res
 }
 
 // Residual rows: top (3V): A x_c + (C^T lam)_c - rhs ; one thread per (c, i),
-// grouped so each A row is read once for the three blocks.
+// grouped so each A row is read once for the three blocks; ctl = C^T lam
+// (precomputed, null when k = 0). res (optional) receives rhs - (A x + C^T lam).
 __global__ void __launch_bounds__(256)
-residual_top_kernel(const double* __restrict__ A, int32_t V, const double* __restrict__ C,
-                    int32_t k, const double* __restrict__ x, const double* __restrict__ lam,
-                    const double* __restrict__ rhs, double* __restrict__ out_res,
-                    double* __restrict__ out_rhs) {
+residual_top_kernel(const double* __restrict__ A, int32_t V, const double* __restrict__ ctl,
+                    const double* __restrict__ x, const double* __restrict__ rhs,
+                    double* __restrict__ out_res, double* __restrict__ out_rhs,
+                    double* __restrict__ res) {
     // one CTA per row i: 256 threads stride the row
     const int32_t i = blockIdx.x;
     const double* Ai = A + (int64_t)i * V;
@@ -531,20 +684,31 @@ residual_top_kernel(const double* __restrict__ A, int32_t V, const double* __res
     s1 = block_sum<256>(s1);
     s2 = block_sum<256>(s2);
     if (threadIdx.x == 0) {
-        const int64_t m = 3 * (int64_t)V;
         double r2 = 0.0, b2 = 0.0;
         double s[3] = {s0, s1, s2};
         for (int c = 0; c < 3; c++) {
             const int64_t row = (int64_t)c * V + i;
             double v = s[c];
-            for (int32_t r = 0; r < k; r++) v += C[(int64_t)r * m + row] * lam[r];
+            if (ctl) v += ctl[row];
             const double d = v - rhs[row];
+            if (res) res[row] = -d;
             r2 += d * d;
             b2 += rhs[row] * rhs[row];
         }
         out_res[i] = r2;
         out_rhs[i] = b2;
     }
+}
+
+// out[row] = sum_r C[r][row] lam[r] (C k x m row-major), r in order.
+__global__ void __launch_bounds__(256)
+ct_lambda_kernel(const double* __restrict__ C, int32_t k, int64_t m, const double* __restrict__ lam,
+                 double* __restrict__ out) {
+    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= m) return;
+    double v = 0.0;
+    for (int32_t r = 0; r < k; r++) v += C[(int64_t)r * m + row] * lam[r];
+    out[row] = v;
 }
 
 inline int32_t grid_for(int64_t n, int bs) { return (int32_t)((n + bs - 1) / bs); }
@@ -573,8 +737,8 @@ int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, doub
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm0));
     TPE_CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-    TPE_CUDA_TRY(cudaFuncSetAttribute(gemm_lower_update_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg));
+    auto update = (n & 1) ? gemm_lower_update_kernel<false> : gemm_lower_update_kernel<true>;
+    TPE_CUDA_TRY(cudaFuncSetAttribute(update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg));
     while ((int32_t)ctx->fac_events.size() < 2 * nsteps + 2) {
         cudaEvent_t e;
         TPE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -604,7 +768,7 @@ int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, doub
             if (kb + 1 < kend) {
                 const int32_t r_s = (kb + 1) * NB, c_e = min(n, kend * NB);
                 dim3 g((c_e - r_s + GT - 1) / GT, (n - r_s + GT - 1) / GT);
-                gemm_lower_update_kernel<<<g, 256, smg, sa>>>(d_L, n, r_s, r_s, c_e, kb * NB, NB);
+                update<<<g, 256, smg, sa>>>(d_L, n, r_s, r_s, c_e, kb * NB, NB);
             }
         }
         TPE_CUDA_TRY(cudaEventRecord(ev[2 * s], sa));
@@ -613,11 +777,11 @@ int32_t cholesky_fp64(tpe_ctx* ctx, double* d_L, double* d_Linv, int32_t n, doub
             const int32_t r_s = kend * NB, c_next = min(n, (kend + OUT) * NB);
             const int32_t k0 = K0b * NB, kl = (kend - K0b) * NB;
             dim3 g1((c_next - r_s + GT - 1) / GT, (n - r_s + GT - 1) / GT);
-            gemm_lower_update_kernel<<<g1, 256, smg, sb>>>(d_L, n, r_s, r_s, c_next, k0, kl);
+            update<<<g1, 256, smg, sb>>>(d_L, n, r_s, r_s, c_next, k0, kl);
             TPE_CUDA_TRY(cudaEventRecord(ev[2 * s + 1], sb));
             if (c_next < n) {
                 dim3 g2((n - c_next + GT - 1) / GT, (n - c_next + GT - 1) / GT);
-                gemm_lower_update_kernel<<<g2, 256, smg, sb>>>(d_L, n, c_next, c_next, n, k0, kl);
+                update<<<g2, 256, smg, sb>>>(d_L, n, c_next, c_next, n, k0, kl);
             }
         }
     }
@@ -772,8 +936,10 @@ int32_t combine_solution(tpe_ctx* ctx, const double* d_w, const double* d_Y, int
 
 int32_t saddle_residual(tpe_ctx* ctx, const double* d_A, int32_t V, const double* d_C, int32_t k,
                         const double* d_x, const double* lam, const double* d_rhs_top,
-                        const double* rhs_bottom, double* out) {
-    TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * (size_t)(2 * V + 16 + k)));
+                        const double* rhs_bottom, double* out, double* d_res_top,
+                        double* res_bottom) {
+    const int64_t m = 3 * (int64_t)V;
+    TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * (size_t)(2 * V + 16 + k + m)));
     TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * (size_t)(k + 3 + 512)));
     double* dl = ctx->scalars.as<double>() + 264;
     if (k > 0)
@@ -781,8 +947,14 @@ int32_t saddle_residual(tpe_ctx* ctx, const double* d_A, int32_t V, const double
                                      ctx->stream));
     double* rr = ctx->tmp.as<double>();
     double* rb = rr + V;
-    { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-    residual_top_kernel<<<V, 256, 0, ctx->stream>>>(d_A, V, d_C, k, d_x, dl, d_rhs_top, rr, rb); }
+    double* ctl = rb + V + 16 + k;
+    {
+        KernelScope ks(ctx, TPE_KGROUP_OTHER, k > 0 ? 2 : 1);
+        if (k > 0)
+            ct_lambda_kernel<<<grid_for(m, 256), 256, 0, ctx->stream>>>(d_C, k, m, dl, ctl);
+        residual_top_kernel<<<V, 256, 0, ctx->stream>>>(d_A, V, k > 0 ? ctl : nullptr, d_x, d_rhs_top,
+                                                        rr, rb, d_res_top);
+    }
     TPE_CUDA_TRY(cudaGetLastError());
     double top_r = 0.0, top_b = 0.0;
     TPE_TRY(dot(ctx, V, rr, nullptr, &top_r));
@@ -790,7 +962,6 @@ int32_t saddle_residual(tpe_ctx* ctx, const double* d_A, int32_t V, const double
     // bottom rows C x - rhs_bottom
     double bot_r = 0.0, bot_b = 0.0;
     if (k > 0) {
-        TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * (size_t)(2 * V + 16 + k)));
         double* cx = ctx->tmp.as<double>() + 2 * V;
         TPE_TRY(gram_dots(ctx, d_C, k, d_x, 1, 3 * (int64_t)V, cx));
         std::vector<double> h((size_t)k);
@@ -800,12 +971,96 @@ int32_t saddle_residual(tpe_ctx* ctx, const double* d_A, int32_t V, const double
         for (int32_t r = 0; r < k; r++) {
             const double b = rhs_bottom ? rhs_bottom[r] : 0.0;
             const double d = h[r] - b;
+            if (res_bottom) res_bottom[r] = -d;
             bot_r += d * d;
             bot_b += b * b;
         }
     }
     const double rn = sqrt(top_r + bot_r), bn = sqrt(top_b + bot_b);
     *out = rn / (bn > 1.0 ? bn : 1.0);
+    return TPE_OK;
+}
+
+int32_t dgemm_nt(tpe_ctx* ctx, const DGemmArgs& g, cudaStream_t stream) {
+    if (g.M <= 0 || g.N <= 0) return TPE_OK;
+    const bool al = ((((uintptr_t)g.A) | ((uintptr_t)g.B)) & 15) == 0 && (g.lda & 1) == 0 &&
+                    (g.ldb & 1) == 0;
+    auto kern = al ? dgemm_nt_kernel<true> : dgemm_nt_kernel<false>;
+    const size_t smem = sizeof(double) * 4 * GT * GP;
+    TPE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((g.N + GT - 1) / GT), (unsigned)((g.M + GT - 1) / GT));
+    kern<<<grid, 256, smem, stream>>>(g);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
+namespace {
+// X[r1.., r1..] for the 64-blocks [b0, b0 + nblk): recursive halving,
+// X21 = -X22 L21 X11 from T^T = W11 L21^T, then W12 = X21^T.
+int32_t inverse_blocks(tpe_ctx* ctx, const double* L, int32_t n, double* X, double* W,
+                       double* Tt, int32_t b0, int32_t nblk, int64_t* launches) {
+    if (nblk <= 1) return TPE_OK;
+    const int32_t h = nblk / 2;
+    TPE_TRY(inverse_blocks(ctx, L, n, X, W, Tt, b0, h, launches));
+    TPE_TRY(inverse_blocks(ctx, L, n, X, W, Tt, b0 + h, nblk - h, launches));
+    const int32_t r1 = b0 * NB, m1 = h * NB, r2 = r1 + m1;
+    const int32_t m2 = min(n, (b0 + nblk) * NB) - r2;
+    DGemmArgs t;  // T^T (m1 x m2) = W11 L21^T
+    t.A = W + (int64_t)r1 * n + r1;
+    t.lda = n;
+    t.B = L + (int64_t)r2 * n + r1;
+    t.ldb = n;
+    t.C = Tt;
+    t.ldc = m2;
+    t.M = m1;
+    t.N = m2;
+    t.K = m1;
+    t.mode = kDAUpper;
+    TPE_TRY(dgemm_nt(ctx, t, ctx->stream));
+    DGemmArgs u;  // X21 (m2 x m1) = -X22 T
+    u.A = X + (int64_t)r2 * n + r2;
+    u.lda = n;
+    u.B = Tt;
+    u.ldb = m2;
+    u.C = X + (int64_t)r2 * n + r1;
+    u.ldc = n;
+    u.M = m2;
+    u.N = m1;
+    u.K = m2;
+    u.alpha = -1.0;
+    u.mode = kDALower;
+    TPE_TRY(dgemm_nt(ctx, u, ctx->stream));
+    transpose_fp64_kernel<<<dim3((m1 + 31) / 32, (m2 + 31) / 32), dim3(32, 8), 0, ctx->stream>>>(
+        X + (int64_t)r2 * n + r1, n, m2, m1, W + (int64_t)r1 * n + r2, n);
+    TPE_CUDA_TRY(cudaGetLastError());
+    *launches += 3;
+    return TPE_OK;
+}
+}  // namespace
+
+int32_t spd_inverse_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
+                         double* X, double* W, double* Tt, double* out) {
+    const int32_t nb = (n + NB - 1) / NB;
+    int64_t launches = 0;
+    KernelScope ks(ctx, TPE_KGROUP_TRSV, 3 + 3 * (int64_t)(nb - 1));
+    TPE_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n * n, ctx->stream));
+    TPE_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * (size_t)n * n, ctx->stream));
+    diag_inverse_kernel<<<nb, 256, 0, ctx->stream>>>(d_Linv, n, X, W);
+    TPE_CUDA_TRY(cudaGetLastError());
+    TPE_TRY(inverse_blocks(ctx, d_L, n, X, W, Tt, 0, nb, &launches));
+    DGemmArgs g;  // out = X^T X = W W^T (lower tiles; W[i][k] = 0 for k < i)
+    g.A = W;
+    g.lda = n;
+    g.B = W;
+    g.ldb = n;
+    g.C = out;
+    g.ldc = n;
+    g.M = g.N = g.K = n;
+    g.mode = kDLowerTiles | kDAUpper;
+    TPE_TRY(dgemm_nt(ctx, g, ctx->stream));
+    const unsigned nt = (unsigned)((n + 31) / 32);
+    mirror_lower_kernel<<<dim3(nt, nt), dim3(32, 8), 0, ctx->stream>>>(out, n);
+    TPE_CUDA_TRY(cudaGetLastError());
     return TPE_OK;
 }
 

@@ -825,6 +825,25 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     return TPE_OK;
 }
 
+int32_t mrhs_fp64(tpe_ctx* ctx, const double* M, int32_t n, const double* X, int32_t ldx,
+                  int32_t nr, double* Y) {
+    if (nr <= 0 || n <= 0) return TPE_OK;
+    if (nr > kMaxRhs || ldx < n) {
+        set_error(ctx, TPE_ERR_TOO_LARGE, "mrhs_fp64: at most 16 right-hand sides, ldx >= n");
+        return TPE_ERR_TOO_LARGE;
+    }
+    constexpr int kSplit = 8;
+    TPE_TRY(ensure(ctx, ctx->mx_part, sizeof(double) * (size_t)kSplit * kMaxRhs * ldx));
+    double* part = ctx->mx_part.as<double>();
+    KernelScope ks(ctx, TPE_KGROUP_OTHER, 2);
+    mrhs_dmma_kernel<0, double><<<dim3((unsigned)((n + kMvRows - 1) / kMvRows), kSplit), 256, 0,
+                                  ctx->stream>>>(M, n, n, X, ldx, nr, part);
+    mrhs_reduce_kernel<<<nblk((int64_t)nr * n, 256), 256, 0, ctx->stream>>>(
+        part, kSplit, n, ldx, nr, nullptr, 0.0, nullptr, Y);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
 // Solves A_rho X = B for nr right-hand sides (B, X: [nr][V] FP64 device; may
 // alias) by CG on the scaled system preconditioned with the FP32 inverse factor.
 // *iters = iterations of the last pass; *converged = every column reached

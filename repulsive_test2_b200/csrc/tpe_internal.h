@@ -65,6 +65,10 @@ struct SaddleOp {
     double* Y = nullptr;     // k x 3V: Abar_rho^{-1} C^T (row s = column s of C^T)
     double* W = nullptr;     // 3V: Abar_rho^{-1} b for the b given at factor time (row k of Y)
     const double* w_src = nullptr;  // that b (device), or null
+    // large constraint sets (schur.cu): explicit inverses on the device
+    bool large = false;
+    double* Ainv = nullptr;  // V x V: A_rho^{-1}
+    double* Sinv = nullptr;  // k x k: (C A3^{-1} C^T)^{-1}
     // host: small Schur complement and its factors
     std::vector<double> Scc;   // k x k, then its Cholesky factor (lower)
     std::vector<double> Scu;   // k x 3 = C U / rho
@@ -126,6 +130,9 @@ struct tpe_ctx {
     tpe::DevBuf pos, pos2, pos3, edge_a, edge_b, grad, edge_acc, partial, scalars, flat0, flat1,
         flat2, flat3, dir;
     tpe::DevBuf grad_ctr;  // tile counter of the SM-bounded gradient kernel
+    // large constraint sets (schur.cu)
+    tpe::DevBuf mat_Ainv, inv_X, inv_W, inv_T, sch_nz, sch_S, sch_L, sch_Linv, sch_Sinv, sch_vec;
+    tpe::DevBuf ref_r, ref_x;  // residual and correction of the refinement step
     tpe::DevBuf mx_ctr;    // tile counters of the persistent trailing updates
     tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
     tpe::DevBuf edge_m;                     // mixed-precision edge records (4 float4 per edge)
@@ -214,6 +221,29 @@ int32_t gram_dots(tpe_ctx* ctx, const double* X, int32_t nx, const double* Y, in
                   int64_t len, double* d_out);
 // A_rho = A + shift (every entry) into L (lower triangle copied), and trace(A) into *d_trace.
 int32_t shift_copy(tpe_ctx* ctx, const double* d_A, double* d_L, int32_t n, double shift);
+// C = alpha A B^T + beta C, FP64 row-major, on the FP64 tensor cores (dense.cu).
+enum : int32_t { kDLowerTiles = 1, kDAUpper = 2, kDALower = 4 };
+struct DGemmArgs {
+    const double* A = nullptr;
+    int64_t lda = 0;
+    const double* B = nullptr;
+    int64_t ldb = 0;
+    double* C = nullptr;
+    int64_t ldc = 0;
+    int32_t M = 0, N = 0, K = 0;
+    double alpha = 1.0, beta = 0.0;
+    int32_t mode = 0;
+};
+int32_t dgemm_nt(tpe_ctx* ctx, const DGemmArgs& g, cudaStream_t stream);
+// out = (L L^T)^{-1}, n x n symmetric, from the Cholesky factor and its 64x64
+// diagonal-block inverses (cholesky_fp64); X, W (n x n) and Tt ((n/2 + 64)^2)
+// are scratch. X = L^{-1} by recursive halving, then out = X^T X.
+int32_t spd_inverse_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
+                         double* X, double* W, double* Tt, double* out);
+// Y[c][i] = sum_j M[i][j] X[c][j] for c < nr <= 16: M n x n FP64 (row length n),
+// X and Y nr rows of stride ldx >= n (mixed.cu: the CG's multi-RHS kernel).
+int32_t mrhs_fp64(tpe_ctx* ctx, const double* M, int32_t n, const double* X, int32_t ldx,
+                  int32_t nr, double* Y);
 int32_t trace(tpe_ctx* ctx, const double* d_A, int32_t n, double* d_out);
 
 // ---- mixed-precision solve (mixed.cu) ------------------------------------
@@ -225,6 +255,18 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
 // FP32 factor as preconditioner, to ||B - A_rho X|| <= tol ||B|| per column.
 int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* d_X, int32_t nr,
                     int32_t maxit, double tol, int32_t* iters, bool* converged);
+
+// ---- large constraint sets (schur.cu) ----------------------------------------
+// Constraint sets with more rows than this take the explicit-inverse Schur path.
+constexpr int32_t kLargeSchur = 64;
+// From the FP64 factor op.L: op.Ainv, op.Y (k x 3V), op.W = A3^{-1} b when b is
+// given, and op.Sinv; *singular when the Schur complement is not SPD.
+int32_t large_schur_build(tpe_ctx* ctx, SaddleOp& op, const double* b_flat, bool* singular);
+// out[c] = Sinv rc[c] for nr host vectors of length k (host in and out).
+int32_t large_schur_apply(tpe_ctx* ctx, const SaddleOp& op, const double* rc, int32_t nr,
+                          double* out);
+// Joins the gradient running on stream3 (api.cu).
+int32_t finish_gradient(tpe_ctx* ctx);
 
 // ---- constraints (constraints.cu) -----------------------------------------
 // Upload the set, returns k (stacked rows).
@@ -254,9 +296,12 @@ int32_t l2_curve_norm(tpe_ctx* ctx, const double* d_vals, const double* d_pos, d
 // x_flat(3V) = w - sum_s Y[s] * lam[s] - U mu / rho ; lam/mu are host arrays
 int32_t combine_solution(tpe_ctx* ctx, const double* d_w, const double* d_Y, int32_t k,
                          const double* lam, const double* mu, double rho, int32_t V, double* d_x);
-// Structured residual ||K z - rhs|| / max(1, ||rhs||) with A (V x V), C (k x 3V).
+// Structured residual ||K z - rhs|| / max(1, ||rhs||) with A (V x V), C (k x 3V);
+// optionally the residual vector rhs - K z itself: top (device, 3V) and bottom
+// (host, k).
 int32_t saddle_residual(tpe_ctx* ctx, const double* d_A, int32_t V, const double* d_C, int32_t k,
                         const double* d_x, const double* lam, const double* d_rhs_top,
-                        const double* rhs_bottom, double* out);
+                        const double* rhs_bottom, double* out, double* d_res_top = nullptr,
+                        double* res_bottom = nullptr);
 
 }  // namespace tpe

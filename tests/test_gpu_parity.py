@@ -230,6 +230,16 @@ def test_step_random_walk_256_vs_oracle():
     _step_compare(v, e, blocks, {"projectionMode": "frozen"}, o)
 
 
+def test_step_random_walk_odd_size_vs_oracle():
+    """V = 301: rows of the V x V factor start on 8- but not 16-byte boundaries
+    (the trailing update then stages them by 8-byte copies); ragged last block."""
+    v, e = F.random_walk_knot(301, seed=4)
+    x0 = T.barycenterTarget(v, e)
+    blocks = [T.barycenterBlock(x0), T.totalLengthBlock(T.totalLength(v, e))]
+    o = O.default_opts(projection_mode=abi.PROJECTION_FROZEN)
+    _step_compare(v, e, blocks, {"projectionMode": "frozen", "precision": "fp64"}, o)
+
+
 def test_step_edge_lengths_and_pins_vs_oracle():
     v, e = F.trefoil(96, jitter=0.01, seed=5)
     x0 = T.barycenterTarget(v, e)
