@@ -231,6 +231,26 @@ int32_t tpe_penalty_gradient(tpe_ctx* ctx, const double* xyz, const tpe_penaltie
                              double* grad);
 
 /* ---- batching (no single reference counterpart: many sobolevStepSet calls) */
+/* A batch of `ncurves` independent curves, one context (streams, buffers) each;
+ * replaces calling sobolevStepSet (src/core/optimizer.ts:231-440) once per
+ * curve. */
+typedef struct tpe_batch tpe_batch;
+tpe_batch* tpe_batch_create(int32_t device, int32_t ncurves, int32_t* status);
+void tpe_batch_destroy(tpe_batch* batch);
+/* Context of curve i (tpe_last_error, or any single-curve call). */
+tpe_ctx* tpe_batch_context(tpe_batch* batch, int32_t i);
+int32_t tpe_batch_set_topology(tpe_batch* batch, int32_t i, const int32_t* edges, int32_t E,
+                               int32_t V);
+/* One tpe_sobolev_step per curve, all curves concurrently (host threads drive
+ * the curves' contexts, largest first; max_threads <= 0: one per host core).
+ * Per curve i: xyz[i] (V_i x 3), sets[i] / nblocks[i], opts[i], xyz_out[i],
+ * stats[i] and status[i] (the step's return code). Returns TPE_OK when every
+ * curve did, else the status of the first failing curve. */
+int32_t tpe_step_batch(tpe_batch* batch, const double* const* xyz,
+                       const tpe_constraint* const* sets, const int32_t* nblocks,
+                       const tpe_step_opts* opts, double* const* xyz_out, tpe_step_stats* stats,
+                       int32_t* status, int32_t max_threads);
+
 /* Energies of `ncurves` curves that share this context's topology (e.g. the K
  * tau-trial candidates of one line search) in one launch: xyz is
  * ncurves x V x 3, energies[ncurves]. */

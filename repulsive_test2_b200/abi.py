@@ -159,6 +159,13 @@ SIGNATURES = {
     "tpe_energy_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(tpe_params),
                                        C.c_void_p, C.c_void_p]),
     "tpe_profile": (C.c_int32, [vp, C.c_int32]),
+    "tpe_batch_create": (vp, [C.c_int32, C.c_int32, ip]),
+    "tpe_batch_destroy": (None, [vp]),
+    "tpe_batch_context": (vp, [vp, C.c_int32]),
+    "tpe_batch_set_topology": (C.c_int32, [vp, C.c_int32, ip, C.c_int32, C.c_int32]),
+    "tpe_step_batch": (C.c_int32, [vp, C.POINTER(dp), C.POINTER(C.POINTER(tpe_constraint)), ip,
+                                   C.POINTER(tpe_step_opts), C.POINTER(dp), C.POINTER(tpe_step_stats), ip,
+                                   C.c_int32]),
     "tpe_profile_read": (C.c_int32, [vp, dp, C.POINTER(C.c_int64)]),
 }
 

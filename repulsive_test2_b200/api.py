@@ -456,6 +456,76 @@ def sobolevStepSet(vertices, edges, disjointPairs, set_, opts=None):
     return res
 
 
+class Batch:
+    """Many independent curves (own topology each), stepped together by
+    ``tpe_step_batch``: one context per curve, curves run concurrently."""
+
+    def __init__(self, curves, device: int = 0):
+        """curves: list of (vertices, edges)."""
+        self.lib = abi.load_library()
+        st = C.c_int32(0)
+        self.ptr = self.lib.tpe_batch_create(device, len(curves), C.byref(st))
+        if not self.ptr:
+            raise TpeError(f"tpe_batch_create({len(curves)} curves) failed with status {st.value}")
+        self.n = len(curves)
+        self.V = []
+        for i, (v, e) in enumerate(curves):
+            e = np.ascontiguousarray(np.asarray(e, dtype=np.int32).reshape(-1, 2))
+            V = int(np.asarray(v).reshape(-1, 3).shape[0])
+            self._check(i, self.lib.tpe_batch_set_topology(self.ptr, i, e.ctypes.data_as(abi.ip), len(e), V),
+                        "tpe_batch_set_topology")
+            self.V.append(V)
+
+    def _check(self, i, status, what):
+        if status == abi.TPE_OK:
+            return
+        msg = self.lib.tpe_last_error(self.lib.tpe_batch_context(self.ptr, i))
+        raise TpeError(f"{what} (curve {i}) failed with status {status}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self.ptr:
+            self.lib.tpe_batch_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, vertices, sets, opts=None, max_threads: int = 0):
+        """One sobolevStepSet per curve: vertices[i] (V_i x 3), sets[i] (blocks),
+        opts (one dict for all curves, or a list). Returns the per-curve results
+        in the form of sobolevStepSet (without timings / descent field)."""
+        n = self.n
+        ins = [_v(v) for v in vertices]
+        outs = [np.zeros_like(v) for v in ins]
+        keep = []
+        arrs = (C.POINTER(abi.tpe_constraint) * n)()
+        nblocks = (C.c_int32 * n)()
+        for i, s_ in enumerate(sets):
+            arr, k = abi.make_set(s_)
+            keep.append((arr, k))
+            arrs[i] = C.cast(arr, C.POINTER(abi.tpe_constraint))
+            nblocks[i] = len(s_)
+        olist = opts if isinstance(opts, (list, tuple)) else [opts or {}] * n
+        oarr = (abi.tpe_step_opts * n)()
+        for i, od in enumerate(olist):
+            oarr[i] = _opts(od)
+        xin = (abi.dp * n)(*[_dp(v) for v in ins])
+        xout = (abi.dp * n)(*[_dp(v) for v in outs])
+        stats = (abi.tpe_step_stats * n)()
+        status = (C.c_int32 * n)()
+        self.lib.tpe_step_batch(self.ptr, xin, arrs, nblocks, oarr, xout, stats, status, max_threads)
+        res = []
+        for i in range(n):
+            self._check(i, status[i], "tpe_step_batch")
+            st = stats[i]
+            res.append({"vertices": outs[i], "energy": st.energy, "accepted": bool(st.accepted),
+                        "converged": bool(st.converged), "stats": _stats_dict(st)})
+        return res
+
+
 def sobolevStep(vertices, edges, disjointPairs, x0, opts=None):
     """optimizer.ts:455-469: barycenter-only set."""
     return sobolevStepSet(vertices, edges, disjointPairs, [barycenterBlock(x0)], opts)
