@@ -1,0 +1,89 @@
+"""The differentiation + network form at full size: 12 random-walk loops of
+1024 vertices joined at 8 Y-junctions (V = 12288), 16 pinned vertices,
+penalties (length w=1, diff w=10, field w=5, X=(0.5,1,0)), edge-length +
+barycenter + point constraints.
+
+The adjoint gradient (tangent-point energy + penalties) against central
+differences along 256 seeded random unit directions (h = 1e-6) with the gate of the
+reference's gradient test, |fd - an| <= 1e-6 + 1e-5 max|an|; then a descent
+trajectory in FP64 and in mixed precision (which takes the FP64 Schur path for
+a constraint set this large, so the two trajectories agree bit for bit): every
+step is accepted or reports a reason, the objective never increases, the pins
+hold and the edge lengths stay within the projection tolerance."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from repulsive_test2_b200 import api as T
+from repulsive_test2_b200 import fixtures as F
+
+pytestmark = pytest.mark.gpu
+
+PEN = {"totalLength": 1.0, "lengthDiff": 10.0, "field": {"weight": 5.0, "X": [0.5, 1.0, 0.0]}}
+
+
+@pytest.fixture(scope="module")
+def network():
+    v, e = F.loop_network(loops=12, n=1024, junctions=8, seed=5)
+    pins = F.seeded_pins(len(v), 16, seed=11)
+    return v, e, pins
+
+
+def _blocks(v, e, pins):
+    b = [T.barycenterBlock(T.barycenterTarget(v, e)), T.edgeLengthsBlock(T.edgeLengths(v, e))]
+    b += [T.pointBlock(int(p), v[p]) for p in pins]
+    return b
+
+
+def test_network_gradient_vs_central_differences(network):
+    v, e, _ = network
+    en, g = T.energyAndGradient(v, e)
+    g = g + T.penaltyGradient(v, e, PEN)
+    ndir, h = 256, 1e-6
+    # unit directions: a step of h in norm (the loops come within ~1e-4 of each
+    # other, so a per-coordinate step of h would put the O(h^2) truncation of
+    # the central difference above the gate)
+    dirs = F.normals(2024, ndir * v.size).reshape(ndir, -1, 3)
+    dirs /= np.linalg.norm(dirs.reshape(ndir, -1), axis=1)[:, None, None]
+    fd = np.empty(ndir)
+    for c0 in range(0, ndir, 64):
+        d = dirs[c0:c0 + 64]
+        curves = np.concatenate([v[None] + h * d, v[None] - h * d], axis=0)
+        es = T.energyBatch(curves, e)
+        ps = np.array([T.penaltyEnergy(x, e, PEN) for x in curves])
+        tot = es + ps
+        fd[c0:c0 + 64] = (tot[:64] - tot[64:]) / (2 * h)
+    an = np.einsum("kvc,vc->k", dirs, g)
+    assert np.max(np.abs(fd - an)) <= 1e-6 + 1e-5 * np.max(np.abs(an))
+
+
+def test_network_descent_fp64_and_mixed(network):
+    v0, e, pins = network
+    blocks = _blocks(v0, e, pins)
+    ell0 = T.edgeLengths(v0, e)
+    nsteps = 6
+    traj = {}
+    for prec in ("fp64", "mixed"):
+        v = v0.copy()
+        obj = T.calculateEnergy(v, e) + T.penaltyEnergy(v, e, PEN)
+        xs = []
+        for _ in range(nsteps):
+            r = T.sobolevStepSet(v, e, None, blocks, {"projectionMode": "frozen", "precision": prec,
+                                                     "penalties": PEN})
+            assert r["accepted"] or "reason" in r["stats"]
+            if not r["accepted"]:
+                break
+            new = T.calculateEnergy(r["vertices"], e) + T.penaltyEnergy(r["vertices"], e, PEN)
+            assert new <= obj
+            obj = new
+            v = r["vertices"]
+            xs.append(v.copy())
+            assert np.max(np.abs(v[pins] - v0[pins])) <= 1e-3
+            ell = T.edgeLengths(v, e)
+            assert np.linalg.norm(ell - ell0) <= 1e-4 * max(1.0, float(np.sum(ell)))
+        traj[prec] = xs
+    assert len(traj["fp64"]) >= 3
+    assert len(traj["mixed"]) == len(traj["fp64"])
+    for a, b in zip(traj["fp64"], traj["mixed"]):
+        assert np.array_equal(a, b)
