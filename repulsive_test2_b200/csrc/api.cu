@@ -21,6 +21,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
+#include <array>
 #include <chrono>
 #include <vector>
 
@@ -261,25 +263,6 @@ __global__ void step_batch_kernel(const double* __restrict__ p, const double* __
 // x = -sum_s Y[s] lam_a[s] - mu_a[c] / (rho sqrt V) (the same operations, in the
 // same order, as combine_kernel) added to the positions cur[a]; bad[a] = 1 when
 // x has a non-finite entry (the trial is then abandoned).
-__global__ void proj_update_kernel(double* __restrict__ cur, int64_t stride,
-                                   const double* __restrict__ Y, int32_t k,
-                                   const double* __restrict__ coef, const int32_t* __restrict__ idx,
-                                   int32_t V, int32_t* __restrict__ bad) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t m = 3 * (int64_t)V;
-    if (t >= m) return;
-    const int a = idx[blockIdx.y];
-    const double* cf = coef + (size_t)blockIdx.y * (k + 3);
-    double v = 0.0;
-    for (int32_t s2 = 0; s2 < k; s2++) v -= Y[(int64_t)s2 * m + t] * cf[s2];
-    const int c = (int)(t / V);
-    v -= cf[k + c];
-    if (!isfinite(v)) bad[a] = 1;
-    const int64_t i = t % V;
-    double* q = cur + (int64_t)a * stride + 3 * i + c;
-    *q = *q + v;
-}
-
 __global__ void step_kernel(const double* __restrict__ p, const double* __restrict__ dir,
                             double tau, int64_t n, double* __restrict__ out) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -618,6 +601,49 @@ int32_t schur_multipliers(tpe_ctx* ctx, const SaddleOp& op, const std::vector<do
     return TPE_OK;
 }
 
+// schur_multipliers for several reduced right-hand sides at once (the trials
+// of a batched projection): with a large constraint set the Sinv products of
+// all of them share one pass over Sinv; otherwise one host solve each.
+int32_t schur_multipliers_multi(tpe_ctx* ctx, const SaddleOp& op,
+                                const std::vector<std::vector<double>>& rcs, const double* ru,
+                                std::vector<std::vector<double>>& lams,
+                                std::vector<std::array<double, 3>>& mus) {
+    const int32_t k = op.k, n = (int32_t)rcs.size();
+    lams.assign((size_t)n, std::vector<double>((size_t)k, 0.0));
+    mus.assign((size_t)n, {0.0, 0.0, 0.0});
+    if (n == 0 || k == 0) return TPE_OK;
+    if (!op.large) {
+        for (int32_t q = 0; q < n; q++) TPE_TRY(schur_multipliers(ctx, op, rcs[q], ru, lams[q], mus[q].data()));
+        return TPE_OK;
+    }
+    std::vector<double> in((size_t)n * k), t((size_t)n * k);
+    for (int32_t q = 0; q < n; q++) std::copy(rcs[q].begin(), rcs[q].end(), in.begin() + (size_t)q * k);
+    TPE_TRY(large_schur_apply(ctx, op, in.data(), n, t.data()));
+    if (!op.trans_constrained) {
+        for (int32_t q = 0; q < n; q++)
+            std::copy(t.begin() + (size_t)q * k, t.begin() + (size_t)(q + 1) * k, lams[q].begin());
+        return TPE_OK;
+    }
+    for (int32_t q = 0; q < n; q++) {
+        const double* tq = t.data() + (size_t)q * k;
+        std::vector<double> rhs(3);
+        for (int c = 0; c < 3; c++) {
+            double s = 0;
+            for (int32_t r = 0; r < k; r++) s += op.Scu[(size_t)r * 3 + c] * tq[r];
+            rhs[c] = s - ru[c];
+        }
+        host_chol_solve(op.M, 3, rhs);
+        for (int c = 0; c < 3; c++) mus[q][c] = rhs[c];
+        double* r2 = in.data() + (size_t)q * k;
+        for (int32_t r = 0; r < k; r++)
+            for (int c = 0; c < 3; c++) r2[r] -= op.Scu[(size_t)r * 3 + c] * mus[q][c];
+    }
+    TPE_TRY(large_schur_apply(ctx, op, in.data(), n, t.data()));
+    for (int32_t q = 0; q < n; q++)
+        std::copy(t.begin() + (size_t)q * k, t.begin() + (size_t)(q + 1) * k, lams[q].begin());
+    return TPE_OK;
+}
+
 // One solve with the current operator: b_flat (device, 3V, or null = 0), d
 // (host, k, or null = 0). x_flat (device) and lam (host) out.
 int32_t op_solve_once(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_flat,
@@ -885,7 +911,9 @@ int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, c
     double* d_coef = d_ns + (size_t)ntrial * 2 * nb;
     std::vector<double> phi((size_t)ntrial * k), ns((size_t)ntrial * 2 * nb);
     std::vector<int32_t> hbad(ntrial, 0);
-    std::vector<double> coef, lam;
+    std::vector<double> coef;
+    std::vector<std::vector<double>> rcs, lams;
+    std::vector<std::array<double, 3>> mus;
     std::vector<int32_t> upd;
     const double ru[3] = {0.0, 0.0, 0.0};
     for (int32_t it = 0; it <= o->proj_max_iter && !active.empty(); it++) {
@@ -904,6 +932,7 @@ int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, c
         std::vector<int32_t> next;
         upd.clear();
         coef.clear();
+        rcs.clear();
         for (int32_t q = 0; q < na; q++) {
             const int32_t a = active[q];
             if (it > 0 && hbad[a]) {  // last correction was not finite
@@ -936,16 +965,19 @@ int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, c
             }
             std::vector<double> rc((size_t)k);
             for (int32_t r = 0; r < k; r++) rc[r] = 0.0 - (-ph[r]);
-            double mu[3];
-            TPE_TRY(schur_multipliers(ctx, op, rc, ru, lam, mu));
-            const double su = 1.0 / (op.rho * sqrt((double)V));
-            for (int32_t r = 0; r < k; r++) coef.push_back(lam[r]);
-            for (int c = 0; c < 3; c++) coef.push_back(mu[c] * su);
+            rcs.push_back(std::move(rc));
             upd.push_back(a);
             next.push_back(a);
         }
         active = next;
         if (upd.empty()) break;
+        // the Newton multipliers of every trial corrected this iteration, together
+        TPE_TRY(schur_multipliers_multi(ctx, op, rcs, ru, lams, mus));
+        const double su = 1.0 / (op.rho * sqrt((double)V));
+        for (size_t q = 0; q < upd.size(); q++) {
+            for (int32_t r = 0; r < k; r++) coef.push_back(lams[q][r]);
+            for (int c = 0; c < 3; c++) coef.push_back(mus[q][c] * su);
+        }
         {
             Timer t(ctx, timings, TPE_PHASE_SADDLE);
             const int32_t nu = (int32_t)upd.size();
@@ -953,10 +985,7 @@ int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, c
                                          cudaMemcpyHostToDevice, ctx->stream));
             TPE_CUDA_TRY(cudaMemcpyAsync(d_coef, coef.data(), sizeof(double) * coef.size(),
                                          cudaMemcpyHostToDevice, ctx->stream));
-            KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-            proj_update_kernel<<<dim3((unsigned)((m + 255) / 256), (unsigned)nu), 256, 0,
-                                 ctx->stream>>>(d_cur, m, op.Y, k, d_coef, d_idx, V, d_bad);
-            TPE_CUDA_TRY(cudaGetLastError());
+            TPE_TRY(project_update(ctx, op.Y, k, V, d_coef, nu, d_idx, d_cur, m, d_bad));
             // the host vectors must outlive the copies
             TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         }
@@ -1232,7 +1261,7 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->mx_Zd, &ctx->mx_Wd, &ctx->grad_ctr, &ctx->mx_ctr, &ctx->mat_Ainv,
                       &ctx->inv_X, &ctx->inv_W, &ctx->inv_T, &ctx->sch_nz, &ctx->sch_S,
                       &ctx->sch_L, &ctx->sch_Linv, &ctx->sch_Sinv, &ctx->sch_vec,
-                      &ctx->ref_r, &ctx->ref_x};
+                      &ctx->ref_r, &ctx->ref_x, &ctx->ycomb_part};
     for (DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     for (auto& p : ctx->prof_pending) {

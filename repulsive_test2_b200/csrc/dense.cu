@@ -650,16 +650,78 @@ __global__ void l2_terms_kernel(const double* __restrict__ vals, const double* _
 }
 
 // x = w - sum_s Y[s] lam[s] - (mu_c / (rho sqrt(V))) in block c.
-__global__ void combine_kernel(const double* __restrict__ w, const double* __restrict__ Y,
-                               int32_t k, const double* __restrict__ coef, int32_t V,
-                               double* __restrict__ x) {
+// Y^T coef for nu <= 16 coefficient vectors (coef[q]: k multipliers, then the
+// 3 scaled mu), Y k x m (block layout), split over ks chunks of rows s:
+// part[ks][q][t] = -sum_{s in chunk ks} Y[s][t] coef[q][s], s in order. The
+// number of chunks depends on k only, so every caller sums in the same order.
+constexpr int kYcMaxQ = 16;
+inline int32_t ycomb_chunks(int32_t k) { return k >= 512 ? min(32, k / 256) : 1; }
+
+__global__ void __launch_bounds__(256)
+ycomb_part_kernel(const double* __restrict__ Y, int32_t k, int64_t m,
+                  const double* __restrict__ coef, int32_t nu, double* __restrict__ part) {
+    constexpr int kChunk = 64;
+    __shared__ double cs[kChunk][kYcMaxQ];
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t ks = blockIdx.y, nks = gridDim.y;
+    const int32_t per = (k + nks - 1) / nks;
+    const int32_t sb = ks * per, se = min(k, sb + per);
+    double v[kYcMaxQ];
+#pragma unroll
+    for (int q = 0; q < kYcMaxQ; q++) v[q] = 0.0;
+    for (int32_t s0 = sb; s0 < se; s0 += kChunk) {
+        const int32_t n = min(kChunk, se - s0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < kChunk * kYcMaxQ; e += blockDim.x) {
+            const int q = e / kChunk, j = e % kChunk;
+            cs[j][q] = (q < nu && j < n) ? coef[(size_t)q * (k + 3) + s0 + j] : 0.0;
+        }
+        __syncthreads();
+        if (t < m) {
+            for (int j = 0; j < n; j++) {
+                const double y = Y[(int64_t)(s0 + j) * m + t];
+#pragma unroll
+                for (int q = 0; q < kYcMaxQ; q++)
+                    if (q < nu) v[q] -= y * cs[j][q];
+            }
+        }
+    }
+    if (t >= m) return;
+    for (int q = 0; q < nu; q++) part[((int64_t)ks * nu + q) * m + t] = v[q];
+}
+
+// x = w - Y^T coef - mu term (one vector, block layout; w may be null).
+__global__ void combine_final_kernel(const double* __restrict__ w, const double* __restrict__ part,
+                                     int32_t nks, int32_t k, const double* __restrict__ coef,
+                                     int32_t V, double* __restrict__ x) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t m = 3 * (int64_t)V;
     if (t >= m) return;
     double v = w ? w[t] : 0.0;
-    for (int32_t s = 0; s < k; s++) v -= Y[(int64_t)s * m + t] * coef[s];
+    for (int32_t ks = 0; ks < nks; ks++) v += part[(int64_t)ks * m + t];
     v -= coef[k + (int32_t)(t / V)];
     x[t] = v;
+}
+
+// cur[idx[q]] (interleaved V x 3) += -Y^T coef[q] - mu term, flagging non-finite
+// corrections in bad[idx[q]]; the same sums as combine_final_kernel with w = 0.
+__global__ void proj_final_kernel(double* __restrict__ cur, int64_t stride,
+                                  const double* __restrict__ part, int32_t nks, int32_t nu,
+                                  int32_t k, const double* __restrict__ coef,
+                                  const int32_t* __restrict__ idx, int32_t V,
+                                  int32_t* __restrict__ bad) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t m = 3 * (int64_t)V;
+    const int q = blockIdx.y;
+    if (t >= m) return;
+    double v = 0.0;
+    for (int32_t ks = 0; ks < nks; ks++) v += part[((int64_t)ks * nu + q) * m + t];
+    const int c = (int)(t / V);
+    v -= coef[(size_t)q * (k + 3) + k + c];
+    const int a = idx[q];
+    if (!isfinite(v)) bad[a] = 1;
+    double* p = cur + (int64_t)a * stride + 3 * (t % V) + c;
+    *p = *p + v;
 }
 
 // Residual rows: top (3V): A x_c + (C^T lam)_c - rhs ; one thread per (c, i),
@@ -926,11 +988,36 @@ int32_t combine_solution(tpe_ctx* ctx, const double* d_w, const double* d_Y, int
     double* dc = ctx->scalars.as<double>() + 264;
     TPE_CUDA_TRY(cudaMemcpyAsync(dc, coef.data(), sizeof(double) * coef.size(),
                                  cudaMemcpyHostToDevice, ctx->stream));
-    KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-    combine_kernel<<<grid_for(3 * (int64_t)V, 256), 256, 0, ctx->stream>>>(d_w, d_Y, k, dc, V,
-                                                                          d_x);
+    const int64_t m = 3 * (int64_t)V;
+    const int32_t nks = ycomb_chunks(k);
+    TPE_TRY(ensure(ctx, ctx->ycomb_part, sizeof(double) * (size_t)nks * kYcMaxQ * m));
+    double* part = ctx->ycomb_part.as<double>();
+    KernelScope ks(ctx, TPE_KGROUP_OTHER, 2);
+    ycomb_part_kernel<<<dim3(grid_for(m, 256), nks), 256, 0, ctx->stream>>>(d_Y, k, m, dc, 1, part);
+    combine_final_kernel<<<grid_for(m, 256), 256, 0, ctx->stream>>>(d_w, part, nks, k, dc, V, d_x);
     TPE_CUDA_TRY(cudaGetLastError());
     TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return TPE_OK;
+}
+
+int32_t project_update(tpe_ctx* ctx, const double* d_Y, int32_t k, int32_t V, const double* d_coef,
+                       int32_t nu, const int32_t* d_idx, double* d_cur, int64_t stride,
+                       int32_t* d_bad) {
+    if (nu <= 0) return TPE_OK;
+    if (nu > kYcMaxQ) {
+        set_error(ctx, TPE_ERR_TOO_LARGE, "project_update: at most 16 trials per update");
+        return TPE_ERR_TOO_LARGE;
+    }
+    const int64_t m = 3 * (int64_t)V;
+    const int32_t nks = ycomb_chunks(k);
+    TPE_TRY(ensure(ctx, ctx->ycomb_part, sizeof(double) * (size_t)nks * kYcMaxQ * m));
+    double* part = ctx->ycomb_part.as<double>();
+    KernelScope ks(ctx, TPE_KGROUP_OTHER, 2);
+    ycomb_part_kernel<<<dim3(grid_for(m, 256), nks), 256, 0, ctx->stream>>>(d_Y, k, m, d_coef, nu,
+                                                                            part);
+    proj_final_kernel<<<dim3(grid_for(m, 256), nu), 256, 0, ctx->stream>>>(
+        d_cur, stride, part, nks, nu, k, d_coef, d_idx, V, d_bad);
+    TPE_CUDA_TRY(cudaGetLastError());
     return TPE_OK;
 }
 

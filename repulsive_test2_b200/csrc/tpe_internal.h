@@ -133,6 +133,7 @@ struct tpe_ctx {
     // large constraint sets (schur.cu)
     tpe::DevBuf mat_Ainv, inv_X, inv_W, inv_T, sch_nz, sch_S, sch_L, sch_Linv, sch_Sinv, sch_vec;
     tpe::DevBuf ref_r, ref_x;  // residual and correction of the refinement step
+    tpe::DevBuf ycomb_part;    // split-over-rows partial sums of Y^T coef
     tpe::DevBuf mx_ctr;    // tile counters of the persistent trailing updates
     tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
     tpe::DevBuf edge_m;                     // mixed-precision edge records (4 float4 per edge)
@@ -296,6 +297,11 @@ int32_t l2_curve_norm(tpe_ctx* ctx, const double* d_vals, const double* d_pos, d
 // x_flat(3V) = w - sum_s Y[s] * lam[s] - U mu / rho ; lam/mu are host arrays
 int32_t combine_solution(tpe_ctx* ctx, const double* d_w, const double* d_Y, int32_t k,
                          const double* lam, const double* mu, double rho, int32_t V, double* d_x);
+// cur[idx[q]] (interleaved, rows stride apart) += -Y^T coef[q] - mu term for nu <= 16
+// device coefficient vectors (k + 3 each), with combine_solution's sums.
+int32_t project_update(tpe_ctx* ctx, const double* d_Y, int32_t k, int32_t V, const double* d_coef,
+                       int32_t nu, const int32_t* d_idx, double* d_cur, int64_t stride,
+                       int32_t* d_bad);
 // Structured residual ||K z - rhs|| / max(1, ||rhs||) with A (V x V), C (k x 3V);
 // optionally the residual vector rhs - K z itself: top (device, 3V) and bottom
 // (host, k).
