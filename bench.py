@@ -44,7 +44,91 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the per-edge, multi-curve batch and network measurements")
+    p.add_argument("--network-steps", type=int, default=10)
     return p.parse_args()
+
+
+def extras(args):
+    """The other workload forms, each timed through the public API (host buffers,
+    wall clock around synchronous calls): per-edge length constraints at V=8192
+    (k = E + 3), a 64-curve batch of uneven sizes, and the 12 x 1024 loop
+    network with pins and penalties."""
+    from repulsive_test2_b200 import api as T
+    from repulsive_test2_b200 import fixtures as F
+
+    out = {}
+    # per-edge length constraints at V=8192
+    v, e = F.random_walk_knot(args.V, seed=1)
+    ell = T.edgeLengths(v, e)
+    blocks = [T.barycenterBlock(T.barycenterTarget(v, e)), T.edgeLengthsBlock(ell)]
+    o = {"projectionMode": "frozen", "precision": "mixed", "trials": 8,
+         "energyBefore": T.calculateEnergy(v, e)}
+    T.sobolevStepSet(v, e, None, blocks, o)
+    t0 = time.perf_counter()
+    r = T.sobolevStepSet(v, e, None, blocks, o)
+    dt = time.perf_counter() - t0
+    o64 = dict(o, precision="fp64", trials=1)
+    r64 = T.sobolevStepSet(v, e, None, blocks, o64)
+    out["per_edge"] = {
+        "workload": f"random-walk knot V=E={args.V}, [barycenter, edgeLengths] (k = {len(ell) + 3}), one step",
+        "ms_per_step": dt * 1e3, "tau": r["stats"]["tau"], "saddle_residual": r["stats"]["residual"],
+        "energy_rel_err_vs_fp64": abs(r["energy"] - r64["energy"]) / abs(r64["energy"]),
+        "vertices_rel_err_vs_fp64": float(np.linalg.norm(r["vertices"] - r64["vertices"]) /
+                                          np.linalg.norm(r64["vertices"])),
+        "path": "explicit FP64 inverses of A_rho and of the k x k Schur complement (k > 64); the mixed "
+                "request takes the same FP64 solve"}
+    # 64-curve batch
+    curves = F.batch_curves(count=64, vmin=256, vmax=4096, seed=3)
+    sets = [[T.barycenterBlock(T.barycenterTarget(cv, ce)), T.totalLengthBlock(T.totalLength(cv, ce))]
+            for cv, ce in curves]
+    ob = {"projectionMode": "frozen", "precision": "mixed", "trials": 8}
+    b = T.Batch(curves)
+    xs = [cv for cv, _ in curves]
+    b.step(xs, sets, ob)
+    t0 = time.perf_counter()
+    nb = 3
+    for _ in range(nb):
+        b.step(xs, sets, ob)
+    dtb = (time.perf_counter() - t0) / nb
+    t0 = time.perf_counter()
+    for (cv, ce), st_ in zip(curves, sets):
+        T.sobolevStepSet(cv, ce, None, st_, ob)
+    dts = time.perf_counter() - t0
+    b.close()
+    out["batch"] = {"workload": "64 curves, V log-uniform in [256, 4096] (trefoil / torus knots / random "
+                                "walks), [barycenter, totalLength], mixed, 8 step sizes per projection batch",
+                    "curve_steps_per_s": 64 / dtb, "ms_per_batch_step": dtb * 1e3,
+                    "sequential_curve_steps_per_s": 64 / dts}
+    # loop network
+    PEN = {"totalLength": 1.0, "lengthDiff": 10.0, "field": {"weight": 5.0, "X": [0.5, 1.0, 0.0]}}
+    nv, ne = F.loop_network(loops=12, n=1024, junctions=8, seed=5)
+    pins = F.seeded_pins(len(nv), 16, seed=11)
+    nbk = [T.barycenterBlock(T.barycenterTarget(nv, ne)), T.edgeLengthsBlock(T.edgeLengths(nv, ne))]
+    nbk += [T.pointBlock(int(p_), nv[p_]) for p_ in pins]
+    net = {"workload": f"12 x 1024 random-walk loops, 8 Y-junctions (V={len(nv)}, E={len(ne)}), 16 pins, "
+                       "penalties (1, 10, 5, X=(0.5,1,0)), [barycenter, edgeLengths, 16 points]",
+           "steps": args.network_steps}
+    finals = {}
+    for prec in ("fp64", "mixed"):
+        x = nv.copy()
+        acc = 0
+        t0 = time.perf_counter()
+        for _ in range(args.network_steps):
+            rr = T.sobolevStepSet(x, ne, None, nbk, {"projectionMode": "frozen", "precision": prec,
+                                                    "penalties": PEN})
+            if rr["accepted"]:
+                x = rr["vertices"]
+                acc += 1
+        dtn = time.perf_counter() - t0
+        finals[prec] = x
+        net[prec] = {"ms_per_step": dtn * 1e3 / max(1, args.network_steps), "accepted": acc,
+                     "energy_last": rr["energy"]}
+    net["mixed_vs_fp64_vertices_rel_err"] = float(np.linalg.norm(finals["mixed"] - finals["fp64"]) /
+                                                  np.linalg.norm(finals["fp64"]))
+    out["network"] = net
+    return out
 
 
 def workload(V):
@@ -496,6 +580,8 @@ def run_repulsive(args):
         "gpu_launches": int(kl_timed[len(groups)]),
         "clocks": clk.summary(),
     }
+    if not args.no_extras and world == 1:
+        out["extras"] = extras(args)
     if not args.no_cpu_baseline and world == 1:
         t_cpu, desc, parts = cpu_step_estimate(v, e, blocks, {}, args.cpu_budget)
         out["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "steps/s", "cores": 1, "kind": "port",
