@@ -214,13 +214,20 @@ __global__ void zero_row_kernel(const double* __restrict__ A, int32_t V,
     }
 }
 
+// out[0] = trace, out[1] = max |diagonal| (NaN if any is NaN), out[2] = number of
+// exactly zero diagonal entries: the only candidates for a zero row, since an
+// assembled A gets a positive diagonal term from every pair that touches a row.
 __global__ void trace_max_kernel(const double* __restrict__ A, int32_t n, double* __restrict__ out) {
     __shared__ double rs[8], rm[8];
+    __shared__ int zc;
+    if (threadIdx.x == 0) zc = 0;
+    __syncthreads();
     double s = 0.0, mx = 0.0;
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const double d = A[(int64_t)i * n + i];
         s += d;
         mx = (d != d || mx != mx) ? NAN : fmax(mx, fabs(d));
+        if (d == 0.0) atomicAdd(&zc, 1);
     }
     for (int o = 16; o > 0; o >>= 1) {
         s += __shfl_down_sync(0xffffffffu, s, o);
@@ -240,6 +247,7 @@ __global__ void trace_max_kernel(const double* __restrict__ A, int32_t n, double
         }
         out[0] = a;
         out[1] = b;
+        out[2] = (double)zc;
     }
 }
 
@@ -370,7 +378,7 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
     TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * 600));
     op.L = ctx->mat_L.as<double>();
     op.Linv = ctx->mat_Linv.as<double>();
-    double tm[2];
+    double tm[3];
     { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
     trace_max_kernel<<<1, 256, 0, ctx->stream>>>(op.A, V, ctx->scalars.as<double>() + 512); }
     TPE_CUDA_TRY(cudaGetLastError());
@@ -381,17 +389,19 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
         return TPE_OK;
     }
     op.rho = rho;
-    // exactly zero rows of K
-    TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
-    TPE_CUDA_TRY(cudaMemsetAsync(ctx->status.as<int32_t>() + 1, 0, sizeof(int32_t), ctx->stream));
-    { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-    zero_row_kernel<<<V, 256, 0, ctx->stream>>>(op.A, V, op.C, k, ctx->status.as<int32_t>() + 1); }
-    TPE_CUDA_TRY(cudaGetLastError());
-    int32_t zr = 0;
-    TPE_TRY(download(ctx, &zr, ctx->status.as<int32_t>() + 1, sizeof(int32_t)));
-    if (zr > 0) {
-        *singular = true;
-        return TPE_OK;
+    // exactly zero rows of K (only rows with a zero diagonal of A can be)
+    if (tm[2] > 0.0) {
+        TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
+        TPE_CUDA_TRY(cudaMemsetAsync(ctx->status.as<int32_t>() + 1, 0, sizeof(int32_t), ctx->stream));
+        { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
+        zero_row_kernel<<<V, 256, 0, ctx->stream>>>(op.A, V, op.C, k, ctx->status.as<int32_t>() + 1); }
+        TPE_CUDA_TRY(cudaGetLastError());
+        int32_t zr = 0;
+        TPE_TRY(download(ctx, &zr, ctx->status.as<int32_t>() + 1, sizeof(int32_t)));
+        if (zr > 0) {
+            *singular = true;
+            return TPE_OK;
+        }
     }
     op.Scc.assign((size_t)k * k, 0.0);
     op.Scu.assign((size_t)k * 3, 0.0);

@@ -193,44 +193,54 @@ __global__ void pair_diag_kernel(const double4* __restrict__ ea, int32_t E, int3
 // A[v][u] = sum_{(I,a) in inc(v)} sum_{(J,b) in inc(u)} (s_a s_b Mb'[I][J] + M0'[I][J]),
 // s_0 = +1 (v is the edge's first vertex), s_1 = -1. Lower-triangle tiles only;
 // each entry is written with its mirror.
-__global__ void gather_A_kernel(const double2* __restrict__ M, int32_t E,
-                                const int32_t* __restrict__ inc_off,
-                                const int32_t* __restrict__ inc, int32_t V, int32_t tiles,
-                                double* __restrict__ A, double* __restrict__ B,
-                                double* __restrict__ B0) {
-    // blockIdx.x enumerates lower-triangular 32x32 tiles (ti >= tj)
+__global__ void __launch_bounds__(1024)
+gather_A_kernel(const double2* __restrict__ M, int32_t E, const int32_t* __restrict__ inc_off,
+                const int32_t* __restrict__ inc, int32_t V, int32_t tiles, double* __restrict__ A,
+                double* __restrict__ B, double* __restrict__ B0) {
+    // blockIdx.x enumerates lower-triangular 32x32 tiles (ti >= tj); the tile is
+    // written along rows, and its mirror (tj, ti) through a shared-memory
+    // transpose, so both stores are coalesced.
+    __shared__ double ta[32][33], tb[32][33], t0[32][33];
     const int32_t t = blockIdx.x;
     int32_t ti = (int32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
     while ((int64_t)ti * (ti + 1) / 2 > t) ti--;
     while ((int64_t)(ti + 1) * (ti + 2) / 2 <= t) ti++;
     const int32_t tj = t - ti * (ti + 1) / 2;
-    const int32_t v = ti * 32 + threadIdx.y;
-    const int32_t u = tj * 32 + threadIdx.x;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int32_t v = ti * 32 + ty;
+    const int32_t u = tj * 32 + tx;
     (void)tiles;
-    if (v >= V || u >= V || u > v) return;
+    const bool ok = v < V && u < V && u <= v;
     double sb = 0.0, s0 = 0.0;
-    for (int32_t p = inc_off[v]; p < inc_off[v + 1]; p++) {
-        const int32_t I = inc[p] >> 1;
-        const double sa = (inc[p] & 1) ? -1.0 : 1.0;
-        const double2* row = M + (int64_t)I * E;
-        for (int32_t q = inc_off[u]; q < inc_off[u + 1]; q++) {
-            const int32_t J = inc[q] >> 1;
-            const double sgn = (inc[q] & 1) ? -sa : sa;
-            const double2 m = row[J];
-            sb += sgn * m.x;
-            s0 += m.y;
+    if (ok) {
+        for (int32_t p = inc_off[v]; p < inc_off[v + 1]; p++) {
+            const int32_t I = inc[p] >> 1;
+            const double sa = (inc[p] & 1) ? -1.0 : 1.0;
+            const double2* row = M + (int64_t)I * E;
+            for (int32_t q = inc_off[u]; q < inc_off[u + 1]; q++) {
+                const int32_t J = inc[q] >> 1;
+                const double sgn = (inc[q] & 1) ? -sa : sa;
+                const double2 m = row[J];
+                sb += sgn * m.x;
+                s0 += m.y;
+            }
         }
     }
-    const double a = sb + s0;
-    A[(int64_t)v * V + u] = a;
-    A[(int64_t)u * V + v] = a;
-    if (B) {
-        B[(int64_t)v * V + u] = sb;
-        B[(int64_t)u * V + v] = sb;
+    ta[ty][tx] = sb + s0;
+    tb[ty][tx] = sb;
+    t0[ty][tx] = s0;
+    __syncthreads();
+    if (ok) {
+        A[(int64_t)v * V + u] = ta[ty][tx];
+        if (B) B[(int64_t)v * V + u] = tb[ty][tx];
+        if (B0) B0[(int64_t)v * V + u] = t0[ty][tx];
     }
-    if (B0) {
-        B0[(int64_t)v * V + u] = s0;
-        B0[(int64_t)u * V + v] = s0;
+    // mirror: entry (row tj*32 + ty, column ti*32 + tx) = value (ti*32 + tx, tj*32 + ty)
+    const int32_t mr = tj * 32 + ty, mc = ti * 32 + tx;
+    if (mc < V && mr < V && mr < mc) {
+        A[(int64_t)mr * V + mc] = ta[tx][ty];
+        if (B) B[(int64_t)mr * V + mc] = tb[tx][ty];
+        if (B0) B0[(int64_t)mr * V + mc] = t0[tx][ty];
     }
 }
 
