@@ -462,33 +462,45 @@ mrhs_dmma_kernel(const MT* __restrict__ M, int32_t ldm, int32_t n,
             xs[jj * kXs + c] = (c < nr && jj < kn) ? X[(size_t)c * ldx + kc + jj] : 0.0;
         }
         __syncthreads();
-        for (int g = 0; g < kn; g += 16) {
-            const int32_t col = kc + g + m4;
-            double a[4];
-            if (rin && vec && col + 3 < ke) {
-                if constexpr (sizeof(MT) == 8) {
-                    const double2 p0 = *reinterpret_cast<const double2*>(mrow + col);
-                    const double2 p1 = *reinterpret_cast<const double2*>(mrow + col + 2);
-                    a[0] = p0.x;
-                    a[1] = p0.y;
-                    a[2] = p1.x;
-                    a[3] = p1.y;
-                } else {
-                    const float4 p0 = *reinterpret_cast<const float4*>(mrow + col);
-                    a[0] = p0.x;
-                    a[1] = p0.y;
-                    a[2] = p0.z;
-                    a[3] = p0.w;
-                }
-            } else {
+        // four 16-column groups per pass: their loads of M are all issued before
+        // the first MMA (the MMA order, and so the sums, are those of one group
+        // at a time)
+        for (int g0 = 0; g0 < kn; g0 += 64) {
+            double a[4][4];
 #pragma unroll
-                for (int t = 0; t < 4; t++) a[t] = (rin && col + t < ke) ? (double)mrow[col + t] : 0.0;
+            for (int u = 0; u < 4; u++) {
+                const int32_t col = kc + g0 + 16 * u + m4;
+                if (g0 + 16 * u < kn && rin && vec && col + 3 < ke) {
+                    if constexpr (sizeof(MT) == 8) {
+                        const double2 p0 = *reinterpret_cast<const double2*>(mrow + col);
+                        const double2 p1 = *reinterpret_cast<const double2*>(mrow + col + 2);
+                        a[u][0] = p0.x;
+                        a[u][1] = p0.y;
+                        a[u][2] = p1.x;
+                        a[u][3] = p1.y;
+                    } else {
+                        const float4 p0 = *reinterpret_cast<const float4*>(mrow + col);
+                        a[u][0] = p0.x;
+                        a[u][1] = p0.y;
+                        a[u][2] = p0.z;
+                        a[u][3] = p0.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 4; t++)
+                        a[u][t] = (g0 + 16 * u < kn && rin && col + t < ke) ? (double)mrow[col + t] : 0.0;
+                }
             }
 #pragma unroll
-            for (int s4 = 0; s4 < 4; s4++) {
-                const double* xr = xs + (g + m4 + s4) * kXs;
-                dmma884(c0a, c0b, a[s4], xr[gq]);
-                dmma884(c1a, c1b, a[s4], xr[8 + gq]);
+            for (int u = 0; u < 4; u++) {
+                const int g = g0 + 16 * u;
+                if (g >= kn) break;
+#pragma unroll
+                for (int s4 = 0; s4 < 4; s4++) {
+                    const double* xr = xs + (g + m4 + s4) * kXs;
+                    dmma884(c0a, c0b, a[u][s4], xr[gq]);
+                    dmma884(c1a, c1b, a[u][s4], xr[8 + gq]);
+                }
             }
         }
     }
