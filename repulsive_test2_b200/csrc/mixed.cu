@@ -681,10 +681,12 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
     int32_t* d_bad = ctx->status.as<int32_t>() + 2;
     TPE_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 2 * sizeof(int32_t), st));
-    // tile counters of the persistent trailing updates, one per panel
-    TPE_TRY(ensure(ctx, ctx->mx_ctr, sizeof(int32_t) * (size_t)(Vp / kT)));
+    // tile counters of the persistent GEMMs: one per panel's trailing update,
+    // then two per inverse level
+    const size_t nctr = (size_t)(Vp / kT) + 64;
+    TPE_TRY(ensure(ctx, ctx->mx_ctr, sizeof(int32_t) * nctr));
     int32_t* d_ctr = ctx->mx_ctr.as<int32_t>();
-    TPE_CUDA_TRY(cudaMemsetAsync(d_ctr, 0, sizeof(int32_t) * (size_t)(Vp / kT), st));
+    TPE_CUDA_TRY(cudaMemsetAsync(d_ctr, 0, sizeof(int32_t) * nctr, st));
     int32_t* d_err = d_bad + 1;
     double* d = ctx->mx_d.as<double>();
     float* S = ctx->mx_S.as<float>();
@@ -792,8 +794,12 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
         int levels = 0;
         for (int32_t m = kT; m < Vp; m *= 2) levels++;
         KernelScope ks(ctx, TPE_KGROUP_TRSV, 3 * (int64_t)levels);
-        for (int32_t m = kT; m < Vp; m *= 2) {
+        int li = 0;
+        for (int32_t m = kT; m < Vp; m *= 2, li++) {
             const int32_t npairs = Vp / (2 * m);
+            // levels of many tiles run persistent (one CTA per SM walking tiles)
+            const bool pers = m >= 1024;
+            int32_t* c_t = d_ctr + Vp / kT + 2 * li;
             tc::GemmArgs t;  // T^T = W11 L21^T
             t.a_zr = t.a_zc = 2 * m;
             t.b_r0 = m;
@@ -802,7 +808,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             t.M = t.N = t.K = m;
             t.mode = tc::kAUpper;
             t.nbatch = npairs;
-            TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T, t, d_err, st));
+            TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T, t, d_err, st, pers ? ctx->num_sms : 0, c_t));
             tc::GemmArgs u;  // Z21 = -Z22 T
             u.a_r0 = u.a_c0 = m;
             u.a_zr = u.a_zc = 2 * m;
@@ -813,7 +819,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             u.mode = tc::kALower;
             u.alpha = -1.0f;
             u.nbatch = npairs;
-            TC_TRY(tc::gemm_nt(mf.Z, mf.T, mf.Z, u, d_err, st));
+            TC_TRY(tc::gemm_nt(mf.Z, mf.T, mf.Z, u, d_err, st, pers ? ctx->num_sms : 0, c_t + 1));
             transpose_block_kernel<<<dim3(m / 32, m / 32, npairs), dim3(32, 8), 0, st>>>(
                 mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, m);
             TPE_CUDA_TRY(cudaGetLastError());
