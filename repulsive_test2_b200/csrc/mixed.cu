@@ -199,6 +199,73 @@ __device__ __forceinline__ void update_tile(float* a, const float* pl, int ti, i
 // one block distance at a time. Reciprocal square roots are the fast
 // approximate ones: the factor is a preconditioner, CG restores FP64 accuracy.
 // *bad = 1 when a pivot is not positive and finite.
+// Off-diagonal 32 x 32 blocks of Z = L^{-1} inside a diagonal block: for each
+// listed pair (a, b), b < a, T = sum_{c=b}^{a-1} L_ac Z_cb, then Z_ab = -Z_aa T
+// (Z_aa lower). 64 threads per pair (8 x 8 threads of 4 x 4 outputs); threads
+// t < nthr of the caller's group, which synchronises on named barrier bar; tsc
+// holds 32 rows (stride kPl) of T per pair.
+__device__ __forceinline__ void group_sync(int bar, int nthr) {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthr) : "memory");
+}
+
+__device__ void offdiag_blocks(const float* __restrict__ a, float* __restrict__ z,
+                               float* __restrict__ tsc, const int* pa, const int* pb, int npairs,
+                               int t, int nthr, int bar) {
+    const int slot = t >> 6;
+    const bool act = slot < npairs;
+    const int tr = (t >> 3) & 7, tc = t & 7;
+    const int bi = act ? pa[slot] : 0, bj = act ? pb[slot] : 0;
+    float acc[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+    if (act) {
+        for (int k = bj * kPw; k < bi * kPw; k++) {
+            float lr[4], zc[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+                lr[x] = a[(bi * kPw + 4 * tr + x) * kLd + k];
+                zc[x] = z[k * kLd + bj * kPw + 4 * tc + x];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) acc[x][y] += lr[x] * zc[y];
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) tsc[(slot * kPw + 4 * tr + x) * kPl + 4 * tc + y] = acc[x][y];
+    }
+    group_sync(bar, nthr);
+    if (act) {
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+        const int rmax = 4 * tr + 3;
+        for (int q = 0; q <= rmax; q++) {
+            float zr[4], tq[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+                zr[x] = z[(bi * kPw + 4 * tr + x) * kLd + bi * kPw + q];
+                tq[x] = tsc[(slot * kPw + q) * kPl + 4 * tc + x];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) acc[x][y] += zr[x] * tq[y];
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++)
+                z[(bi * kPw + 4 * tr + x) * kLd + bj * kPw + 4 * tc + y] = -acc[x][y];
+    }
+    group_sync(bar, nthr);
+}
+
 __global__ void __launch_bounds__(256, 2)
 potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __restrict__ Zhi,
                 float* __restrict__ Zlo, int32_t* __restrict__ bad) {
@@ -207,6 +274,7 @@ potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __re
     float* z = a + kT * kLd;        // L^{-1} (lower)
     float* pl = z + kT * kLd;       // 96 x 33 panel rows / block products
     float* rd = pl + 96 * kPl;      // 1 / L_ii
+    float* tsc = rd + kT;           // 2 x 32 x 33: T of the off-diagonal blocks done in the loop
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     {
         // whole block, 16-byte loads (ld and j0 are multiples of 128)
@@ -274,70 +342,24 @@ potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __re
                 const int r = e >> 5, m = e & 31;
                 a[(base + r) * kLd + c0 + m] = pl[r * kPl + m];
             }
+            // while warp 0 factors the next panel: the off-diagonal Z blocks of
+            // block row p, whose inputs (L columns < 32 p, Z blocks of rows
+            // <= p) are final
+            if (p > 0) {
+                int pa[2], pb[2];
+                for (int q = 0; q < p; q++) {
+                    pa[q] = p;
+                    pb[q] = p - 1 - q;
+                }
+                offdiag_blocks(a, z, tsc, pa, pb, p, tid - 32, 224, 1);
+            }
         }
         __syncthreads();
     }
-    // off-diagonal blocks of Z: T = sum_{c=b}^{a-1} L_ac Z_cb, then Z_ab = -Z_aa T
-    for (int d = 1; d < kT / kPw; d++) {
-        const int nbk = kT / kPw - d;
-        const int ntl = nbk * 64;  // 4 x 4 tiles of the nbk output blocks
-        float acc[4][4];
-        int bb = 0, tr = 0, tc = 0;
-        const bool act = tid < ntl;
-        if (act) {
-            bb = tid >> 6;
-            tr = (tid >> 3) & 7;
-            tc = tid & 7;
-        }
-        const int bi = bb + d, bj = bb;
-#pragma unroll
-        for (int x = 0; x < 4; x++)
-#pragma unroll
-            for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
-        if (act) {
-            for (int k = bj * kPw; k < bi * kPw; k++) {
-                float lr[4], zc[4];
-#pragma unroll
-                for (int x = 0; x < 4; x++) {
-                    lr[x] = a[(bi * kPw + 4 * tr + x) * kLd + k];
-                    zc[x] = z[k * kLd + bj * kPw + 4 * tc + x];
-                }
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] += lr[x] * zc[y];
-            }
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) pl[(bb * kPw + 4 * tr + x) * kPl + 4 * tc + y] = acc[x][y];
-        }
-        __syncthreads();
-        if (act) {
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
-            const int rmax = 4 * tr + 3;
-            for (int q = 0; q <= rmax; q++) {
-                float zr[4], tq[4];
-#pragma unroll
-                for (int x = 0; x < 4; x++) {
-                    zr[x] = z[(bi * kPw + 4 * tr + x) * kLd + bi * kPw + q];
-                    tq[x] = pl[(bb * kPw + q) * kPl + 4 * tc + x];
-                }
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] += zr[x] * tq[y];
-            }
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++)
-                    z[(bi * kPw + 4 * tr + x) * kLd + bj * kPw + 4 * tc + y] = -acc[x][y];
-        }
-        __syncthreads();
+    // the last block row of Z: its three off-diagonal blocks at once
+    {
+        const int pa[3] = {3, 3, 3}, pb[3] = {2, 1, 0};
+        offdiag_blocks(a, z, pl, pa, pb, 3, tid, 256, 2);
     }
     // Z_jj (split): lane = column, coalesced rows
     for (int e = tid; e < kT * kT; e += 256) {
@@ -702,7 +724,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
         }
     }
     const int nb = Vp / kT;
-    const size_t potrf_smem = sizeof(float) * (2 * kT * kLd + 96 * kPl + kT);
+    const size_t potrf_smem = sizeof(float) * (2 * kT * kLd + 96 * kPl + kT + 2 * kPw * kPl);
     TPE_CUDA_TRY(cudaFuncSetAttribute(potrf128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)potrf_smem));
     // Look-ahead: after panel j is solved (trsm), the main stream updates only
