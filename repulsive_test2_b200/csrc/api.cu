@@ -1236,6 +1236,7 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
     if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->stream3, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->stream4, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_prep, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_grad, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;
@@ -1258,6 +1259,7 @@ void tpe_destroy(tpe_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
     if (ctx->stream3) cudaStreamSynchronize(ctx->stream3);
+    if (ctx->stream4) cudaStreamSynchronize(ctx->stream4);
     DevBuf* bufs[] = {&ctx->d_edges, &ctx->d_inc_off, &ctx->d_inc, &ctx->pos, &ctx->pos2,
                       &ctx->pos3, &ctx->edge_a, &ctx->edge_b, &ctx->grad, &ctx->edge_acc,
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
@@ -1267,7 +1269,7 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status,
                       &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
                       &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,
-                      &ctx->mx_Wlo, &ctx->mx_Thi, &ctx->mx_Tlo, &ctx->mx_vec, &ctx->mx_part,
+                      &ctx->mx_Wlo, &ctx->mx_Thi, &ctx->mx_Tlo, &ctx->mx_T2hi, &ctx->mx_T2lo, &ctx->mx_vec, &ctx->mx_part,
                       &ctx->mx_Zd, &ctx->mx_Wd, &ctx->grad_ctr, &ctx->mx_ctr, &ctx->mat_Ainv,
                       &ctx->inv_X, &ctx->inv_W, &ctx->inv_T, &ctx->sch_nz, &ctx->sch_S,
                       &ctx->sch_L, &ctx->sch_Linv, &ctx->sch_Sinv, &ctx->sch_vec,
@@ -1282,6 +1284,7 @@ void tpe_destroy(tpe_ctx* ctx) {
     for (cudaEvent_t e : ctx->fac_events) cudaEventDestroy(e);
     if (ctx->ev_prep) cudaEventDestroy(ctx->ev_prep);
     if (ctx->ev_grad) cudaEventDestroy(ctx->ev_grad);
+    if (ctx->stream4) cudaStreamDestroy(ctx->stream4);
     if (ctx->stream3) cudaStreamDestroy(ctx->stream3);
     if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     cudaStreamDestroy(ctx->stream);

@@ -372,11 +372,12 @@ potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __re
     }
 }
 
-// W_jj = Z_jj^T for every diagonal block (blockIdx.z = block), split.
+// W_jj = Z_jj^T for the diagonal blocks b0 + blockIdx.z, split.
 __global__ void diag_transpose_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
-                                      float* __restrict__ whi, float* __restrict__ wlo, int32_t ld) {
+                                      float* __restrict__ whi, float* __restrict__ wlo, int32_t ld,
+                                      int32_t b0) {
     __shared__ float th[32][33], tl[32][33];
-    const int32_t j0 = blockIdx.z * kT;
+    const int32_t j0 = (b0 + (int32_t)blockIdx.z) * kT;
     const int32_t r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
     for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
         const size_t o = (size_t)(j0 + r0 + yy) * ld + j0 + c0 + threadIdx.x;
@@ -391,12 +392,12 @@ __global__ void diag_transpose_kernel(const float* __restrict__ zhi, const float
     }
 }
 
-// W[s + c][s + m + r] = Z[s + m + r][s + c] (r, c < m), s = blockIdx.z * 2m.
+// W[s + c][s + m + r] = Z[s + m + r][s + c] (r, c < m), s = base + blockIdx.z * 2m.
 __global__ void transpose_block_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
                                        float* __restrict__ whi, float* __restrict__ wlo,
-                                       int32_t ld, int32_t m) {
+                                       int32_t ld, int32_t m, int32_t base) {
     __shared__ float th[32][33], tl[32][33];
-    const int32_t s = blockIdx.z * 2 * m;
+    const int32_t s = base + (int32_t)blockIdx.z * 2 * m;
     const int32_t r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
     for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
         const size_t o = (size_t)(s + m + r0 + yy) * ld + s + c0 + threadIdx.x;
@@ -681,6 +682,57 @@ int32_t mixed_padded_size(int32_t V) {
 
 // FP32 factorization and inverse of the scaled A_rho (steps 1-3 above).
 // *ok = false when the FP32 factorization broke down.
+namespace {
+// The diagonal transposes and the recursive-halving levels m = 128 .. hs/2 of
+// Z = L^{-1} on the rows [base, base + hs) (hs a power of two times 128), on
+// stream s. The level of width m pairs its blocks two by two: T^T = W11 L21^T
+// (into T rows base/2 + ...), Z21 = -Z22 T, W12 = Z21^T. ctr: two zeroed tile
+// counters per level.
+int32_t inverse_half(tpe_ctx* ctx, int32_t base, int32_t hs, cudaStream_t s, int32_t* d_err,
+                     int32_t* ctr) {
+    MixedFactor& mf = ctx->mf;
+    const int32_t Vp = mf.Vp;
+    diag_transpose_kernel<<<dim3(kT / 32, kT / 32, hs / kT), dim3(32, 8), 0, s>>>(
+        mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, base / kT);
+    TPE_CUDA_TRY(cudaGetLastError());
+    int li = 0;
+    for (int32_t m = kT; m < hs; m *= 2, li++) {
+        const int32_t npairs = hs / (2 * m);
+        const bool pers = m >= 1024 && s == ctx->stream;  // beside the factorization: one tile per CTA
+        tc::GemmArgs t;  // T^T = W11 L21^T
+        t.a_r0 = t.a_c0 = base;
+        t.a_zr = t.a_zc = 2 * m;
+        t.b_r0 = base + m;
+        t.b_c0 = base;
+        t.b_zr = t.b_zc = 2 * m;
+        t.c_r0 = base / 2;
+        t.c_zr = m;
+        t.M = t.N = t.K = m;
+        t.mode = tc::kAUpper;
+        t.nbatch = npairs;
+        TPE_CUDA_TRY(tc::gemm_nt(mf.W, mf.L, mf.T, t, d_err, s, pers ? ctx->num_sms : 0, ctr + 2 * li));
+        tc::GemmArgs u;  // Z21 = -Z22 T
+        u.a_r0 = u.a_c0 = base + m;
+        u.a_zr = u.a_zc = 2 * m;
+        u.b_r0 = base / 2;
+        u.b_zr = m;
+        u.c_r0 = base + m;
+        u.c_c0 = base;
+        u.c_zr = u.c_zc = 2 * m;
+        u.M = u.N = u.K = m;
+        u.mode = tc::kALower;
+        u.alpha = -1.0f;
+        u.nbatch = npairs;
+        TPE_CUDA_TRY(tc::gemm_nt(mf.Z, mf.T, mf.Z, u, d_err, s, pers ? ctx->num_sms : 0,
+                                 ctr + 2 * li + 1));
+        transpose_block_kernel<<<dim3(m / 32, m / 32, npairs), dim3(32, 8), 0, s>>>(
+            mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, m, base);
+        TPE_CUDA_TRY(cudaGetLastError());
+    }
+    return TPE_OK;
+}
+}  // namespace
+
 int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, bool* ok) {
     MixedFactor& mf = ctx->mf;
     *ok = false;
@@ -697,7 +749,10 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     TPE_TRY(make_split(ctx, ctx->mx_Lhi, ctx->mx_Llo, Vp, Vp, mf.L));
     TPE_TRY(make_split(ctx, ctx->mx_Zhi, ctx->mx_Zlo, Vp, Vp, mf.Z));
     TPE_TRY(make_split(ctx, ctx->mx_Whi, ctx->mx_Wlo, Vp, Vp, mf.W));
-    if (Vp > kT) TPE_TRY(make_split(ctx, ctx->mx_Thi, ctx->mx_Tlo, Vp / 2, Vp / 2, mf.T));
+    if (Vp > kT) {
+        TPE_TRY(make_split(ctx, ctx->mx_Thi, ctx->mx_Tlo, Vp / 2, Vp / 2, mf.T));
+        TPE_TRY(make_split(ctx, ctx->mx_T2hi, ctx->mx_T2lo, Vp / 2, Vp / 2, mf.T2));
+    }
     TPE_TRY(ensure(ctx, ctx->mx_Zd, sizeof(float) * (size_t)Vp * Vp));
     TPE_TRY(ensure(ctx, ctx->mx_Wd, sizeof(float) * (size_t)Vp * Vp));
     TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
@@ -739,6 +794,8 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     }
     cudaEvent_t* ev_t = ctx->fac_events.data();        // trsm of panel j done
     cudaEvent_t* ev_r = ctx->fac_events.data() + nb;   // rest of panel j done
+    cudaEvent_t ev_mid = ctx->fac_events[2 * nb];      // panels 0 .. nb/2-1 done
+    cudaEvent_t ev_half = ctx->fac_events[2 * nb + 1]; // first half of the inverse done
     const cudaStream_t st2 = ctx->stream2;
     // The trailing updates run persistent (one CTA per SM walking its tiles) on
     // the SMs left by the concurrent gradient, minus a few kept free so that the
@@ -746,7 +803,10 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     const int32_t rest_ctas = std::max(16, ctx->num_sms - ctx->grad_sms - 8);
     {
         const int64_t nrest = nb > 2 ? nb - 2 : 0;
-        KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + 3 * (int64_t)(nb - 1) + nrest);
+        int sub_h = 0;  // inverse levels of the first half (stream4, below)
+        for (int32_t m = kT; m < Vp / 2; m *= 2) sub_h++;
+        KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + 3 * (int64_t)(nb - 1) + nrest +
+                                                     (nb > 1 ? 2 + 3 * (int64_t)sub_h : 0));
         jacobi_kernel<<<nblk(Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, ctx->mx_dinv.as<double>());
         scale_to_f32_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, S);
         TPE_CUDA_TRY(cudaGetLastError());
@@ -771,6 +831,20 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             t.N = kT;
             t.K = kT;
             TC_TRY(tc::gemm_nt(mf.L, mf.Z, mf.L, t, d_err, st));
+            if (nb > 1 && j == nb / 2 - 1) {
+                // panels 0 .. nb/2-1 are final: the first half of the inverse and
+                // the top level's T^T = W11 L21^T go to stream4 (low priority)
+                TPE_CUDA_TRY(cudaEventRecord(ev_mid, st));
+                TPE_CUDA_TRY(cudaStreamWaitEvent(ctx->stream4, ev_mid, 0));
+                const int32_t H = Vp / 2;
+                TPE_TRY(inverse_half(ctx, 0, H, ctx->stream4, d_err, d_ctr + Vp / kT));
+                tc::GemmArgs t2;  // T^T (H x H) = W11 L21^T
+                t2.b_r0 = H;
+                t2.M = t2.N = t2.K = H;
+                t2.mode = tc::kAUpper;
+                TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T2, t2, d_err, ctx->stream4));
+                TPE_CUDA_TRY(cudaEventRecord(ev_half, ctx->stream4));
+            }
             if (rows > kT) {
                 // rest: S[j0+256.., j0+256..] -= L21 L21^T on lower tiles (low priority stream)
                 TPE_CUDA_TRY(cudaEventRecord(ev_t[j], st));
@@ -806,44 +880,32 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
         if (last_rest >= 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[last_rest], 0));
     }
     {
-        KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
-        diag_transpose_kernel<<<dim3(kT / 32, kT / 32, nb), dim3(32, 8), 0, st>>>(
-            mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp);
-        TPE_CUDA_TRY(cudaGetLastError());
-    }
-    {
-        // Z = L^{-1} level by level (W = Z^T alongside)
-        int levels = 0;
-        for (int32_t m = kT; m < Vp; m *= 2) levels++;
-        KernelScope ks(ctx, TPE_KGROUP_TRSV, 3 * (int64_t)levels);
-        int li = 0;
-        for (int32_t m = kT; m < Vp; m *= 2, li++) {
-            const int32_t npairs = Vp / (2 * m);
-            // levels of many tiles run persistent (one CTA per SM walking tiles)
-            const bool pers = m >= 1024;
-            int32_t* c_t = d_ctr + Vp / kT + 2 * li;
-            tc::GemmArgs t;  // T^T = W11 L21^T
-            t.a_zr = t.a_zc = 2 * m;
-            t.b_r0 = m;
-            t.b_zr = t.b_zc = 2 * m;
-            t.c_zr = m;
-            t.M = t.N = t.K = m;
-            t.mode = tc::kAUpper;
-            t.nbatch = npairs;
-            TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T, t, d_err, st, pers ? ctx->num_sms : 0, c_t));
-            tc::GemmArgs u;  // Z21 = -Z22 T
-            u.a_r0 = u.a_c0 = m;
-            u.a_zr = u.a_zc = 2 * m;
-            u.b_zr = m;
-            u.c_r0 = m;
-            u.c_zr = u.c_zc = 2 * m;
-            u.M = u.N = u.K = m;
+        // Z = L^{-1} (W = Z^T alongside) by recursive halving. The first half
+        // (rows < Vp/2: its diagonal transposes, its levels and the top level's
+        // T^T = W11 L21^T) depends only on panels 0 .. nb/2-1, so it already ran
+        // on stream4 beside the second half of the factorization; the second half
+        // and the top level's Z21 = -Z22 T follow here.
+        int sub = 0;  // levels below the top one
+        for (int32_t m = kT; m < Vp / 2; m *= 2) sub++;
+        KernelScope ks(ctx, TPE_KGROUP_TRSV, Vp > kT ? 3 + 3 * (int64_t)sub : 1);
+        if (Vp == kT) {
+            diag_transpose_kernel<<<dim3(kT / 32, kT / 32, 1), dim3(32, 8), 0, st>>>(
+                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, 0);
+            TPE_CUDA_TRY(cudaGetLastError());
+        } else {
+            const int32_t H = Vp / 2;
+            TPE_TRY(inverse_half(ctx, H, H, st, d_err, d_ctr + Vp / kT + 32));
+            TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_half, 0));
+            tc::GemmArgs u;  // top level: Z21 = -Z22 T
+            u.a_r0 = u.a_c0 = H;
+            u.c_r0 = H;
+            u.M = u.N = u.K = H;
             u.mode = tc::kALower;
             u.alpha = -1.0f;
-            u.nbatch = npairs;
-            TC_TRY(tc::gemm_nt(mf.Z, mf.T, mf.Z, u, d_err, st, pers ? ctx->num_sms : 0, c_t + 1));
-            transpose_block_kernel<<<dim3(m / 32, m / 32, npairs), dim3(32, 8), 0, st>>>(
-                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, m);
+            TC_TRY(tc::gemm_nt(mf.Z, mf.T2, mf.Z, u, d_err, st, H >= 1024 ? ctx->num_sms : 0,
+                               d_ctr + Vp / kT + 63));
+            transpose_block_kernel<<<dim3(H / 32, H / 32, 1), dim3(32, 8), 0, st>>>(
+                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, H, 0);
             TPE_CUDA_TRY(cudaGetLastError());
         }
     }

@@ -81,7 +81,7 @@ struct MixedFactor {
     bool valid = false;
     int V = 0, Vp = 0;
     double rho = 0.0;
-    tc::SplitMat L, Z, W, T;
+    tc::SplitMat L, Z, W, T, T2;  // T: level scratch; T2: the top level's T^T
     tc::SplitMat S;  // plain FP32 trailing matrix (hi only)
 };
 
@@ -102,6 +102,7 @@ struct tpe_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;           // look-ahead stream of the factorization
     cudaStream_t stream3 = nullptr;           // the gradient, concurrent with assembly + factor
+    cudaStream_t stream4 = nullptr;           // first half of the mixed inverse, beside the factor
     cudaEvent_t ev_prep = nullptr, ev_grad = nullptr;
     // a gradient launched on stream3 and not yet joined (step_impl / finish_gradient)
     bool grad_pending = false;
@@ -144,6 +145,7 @@ struct tpe_ctx {
     tpe::DevBuf trial_raw, trial_cur;       // batched line-search trials (K x 3V each)
     tpe::SaddleOp op;
     // mixed-precision factor (mixed.cu)
+    tpe::DevBuf mx_T2hi, mx_T2lo;
     tpe::DevBuf mx_d, mx_dinv, mx_S, mx_Lhi, mx_Llo, mx_Zhi, mx_Zlo, mx_Whi, mx_Wlo, mx_Thi, mx_Tlo,
         mx_vec, mx_part, mx_Zd, mx_Wd;
     tpe::MixedFactor mf;
