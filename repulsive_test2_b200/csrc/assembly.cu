@@ -25,10 +25,6 @@ namespace tpe {
 namespace {
 
 
-__device__ __forceinline__ bool disjoint(int2 a, int2 b) {
-    return a.x != b.x && a.x != b.y && a.y != b.x && a.y != b.y;
-}
-
 // (|d|+eps)^(-(2 sigma + 1)); MODE 1: alpha = 3, beta = 6 -> exponent 7/3.
 template <int MODE>
 __device__ __forceinline__ double inv_dist_pow(double dn, double distExp) {
@@ -260,7 +256,7 @@ int32_t gather_A_launch(tpe_ctx* ctx, double* d_A, double* d_B, double* d_B0) {
 
 int32_t assemble_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_A,
                       double* d_B, double* d_B0) {
-    const int32_t E = ctx->E, V = ctx->V;
+    const int32_t E = ctx->E;
     TPE_TRY(ensure(ctx, ctx->pairM, sizeof(double2) * (size_t)E * E));
     const double s = (beta - 1.0) / alpha;
     const double sigma = s - 1.0;
@@ -284,7 +280,6 @@ int32_t assemble_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, doubl
         TPE_CUDA_TRY(cudaGetLastError());
     }
     return gather_A_launch(ctx, d_A, d_B, d_B0);
-    return TPE_OK;
 }
 
 }  // namespace tpe
