@@ -7,7 +7,8 @@ drift removal, total length 10), tangent-point alpha=3, beta=6, eps=1e-10,
 constraint set [barycenter, totalLength] frozen at the initial curve, frozen
 projection (the app's default), analytical dE. One step = one sobolevStepSet
 (gradient, Gram assembly, structured saddle solve, Armijo line search with
-back-projection) from the same input curve.
+back-projection); the timed loop is a descent trajectory, each step starting at
+the previous step's output.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl repulsive|reference]
 
@@ -32,6 +33,22 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 METRIC = "descent steps/s at V=8192: mixed+batched vs plain FP64 GPU, at <=1e-8 rel energy err"
+
+
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time, on every rank (ms itself without a process group)."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(steps, world, ms):
+    """Whole-job throughput of `world` replicas: every rank's steps over the max time."""
+    return world * steps / (ms * 1e-3)
 
 
 def parse():
@@ -388,12 +405,7 @@ def run_repulsive(args):
         dev_trajectory(o, nsteps, log)
         t1.record(stream)
         torch.cuda.synchronize(dev)
-        ms = t0.elapsed_time(t1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(t0.elapsed_time(t1), dist, dev)
 
     o_mix = step_opts(T, args.precision)
     o_64 = step_opts(T, "fp64")
@@ -443,11 +455,7 @@ def run_repulsive(args):
     host_trajectory(o_mix, args.steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
 
     # accuracy of the mixed step against the FP64 step from the initial curve
     acc = {}
@@ -538,9 +546,9 @@ def run_repulsive(args):
                           "without them")
     roof["group_launches"] = {g: int(nl[g]) for g in groups}
 
-    value = world * steps / (ms * 1e-3)
-    value64 = world * steps / (ms64 * 1e-3)
-    e2e_value = world * steps / (e2e_ms * 1e-3)
+    value = replica_value(steps, world, ms)
+    value64 = replica_value(steps, world, ms64)
+    e2e_value = replica_value(steps, world, e2e_ms)
 
     def traj(log):
         return {"accepted": sum(x["accepted"] for x in log),
