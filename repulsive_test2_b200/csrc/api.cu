@@ -1237,6 +1237,7 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
         cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->stream3, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->stream4, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->stream5, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_prep, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_grad, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;
@@ -1260,6 +1261,7 @@ void tpe_destroy(tpe_ctx* ctx) {
     if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
     if (ctx->stream3) cudaStreamSynchronize(ctx->stream3);
     if (ctx->stream4) cudaStreamSynchronize(ctx->stream4);
+    if (ctx->stream5) cudaStreamSynchronize(ctx->stream5);
     DevBuf* bufs[] = {&ctx->d_edges, &ctx->d_inc_off, &ctx->d_inc, &ctx->pos, &ctx->pos2,
                       &ctx->pos3, &ctx->edge_a, &ctx->edge_b, &ctx->grad, &ctx->edge_acc,
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
@@ -1284,6 +1286,7 @@ void tpe_destroy(tpe_ctx* ctx) {
     for (cudaEvent_t e : ctx->fac_events) cudaEventDestroy(e);
     if (ctx->ev_prep) cudaEventDestroy(ctx->ev_prep);
     if (ctx->ev_grad) cudaEventDestroy(ctx->ev_grad);
+    if (ctx->stream5) cudaStreamDestroy(ctx->stream5);
     if (ctx->stream4) cudaStreamDestroy(ctx->stream4);
     if (ctx->stream3) cudaStreamDestroy(ctx->stream3);
     if (ctx->stream2) cudaStreamDestroy(ctx->stream2);

@@ -782,59 +782,107 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     const size_t potrf_smem = sizeof(float) * (2 * kT * kLd + 96 * kPl + kT + 2 * kPw * kPl);
     TPE_CUDA_TRY(cudaFuncSetAttribute(potrf128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)potrf_smem));
-    // Look-ahead: after panel j is solved (trsm), the main stream updates only
-    // the next block column (strip) and moves on to factor it, while the low
-    // priority stream applies panel j to the rest of the trailing matrix. The
-    // strip of step j and the rest of step j-1 write the same block column, so
-    // the strip waits for that rest.
-    while ((int32_t)ctx->fac_events.size() < 2 * nb + 2) {
+    // Critical path on the main stream, per block j: potrf, split copy of the
+    // panel, the panel solve of its first row tile only (L_{j+1,j}) and the
+    // update of the next diagonal block by it; then potrf j+1. Beside it, on
+    // stream5 (high priority), the rest of the panel solve and the update of the
+    // rest of block column j+1 (which the next split copy waits for), and on
+    // stream2 (low priority) the trailing update of everything to the right.
+    // Every tile receives its updates in the order of the one-stream schedule
+    // (rests of earlier panels first), so the results do not depend on it.
+    while ((int32_t)ctx->fac_events.size() < 4 * nb + 3) {
         cudaEvent_t e;
         TPE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->fac_events.push_back(e);
     }
-    cudaEvent_t* ev_t = ctx->fac_events.data();        // trsm of panel j done
-    cudaEvent_t* ev_r = ctx->fac_events.data() + nb;   // rest of panel j done
-    cudaEvent_t ev_mid = ctx->fac_events[2 * nb];      // panels 0 .. nb/2-1 done
-    cudaEvent_t ev_half = ctx->fac_events[2 * nb + 1]; // first half of the inverse done
-    const cudaStream_t st2 = ctx->stream2;
+    cudaEvent_t* ev_t1 = ctx->fac_events.data();          // first row tile of panel j solved
+    cudaEvent_t* ev_tr = ctx->fac_events.data() + nb;     // whole panel j solved
+    cudaEvent_t* ev_s = ctx->fac_events.data() + 2 * nb;  // block column j+1 final below block j+1
+    cudaEvent_t* ev_r = ctx->fac_events.data() + 3 * nb;  // trailing update of panel j done
+    cudaEvent_t ev_mid = ctx->fac_events[4 * nb];         // panels 0 .. nb/2-1 done
+    cudaEvent_t ev_half = ctx->fac_events[4 * nb + 1];    // first half of the inverse done
+    cudaEvent_t ev_side = ctx->fac_events[4 * nb + 2];    // side streams drained
+    const cudaStream_t st2 = ctx->stream2, st5 = ctx->stream5;
     // The trailing updates run persistent (one CTA per SM walking its tiles) on
     // the SMs left by the concurrent gradient, minus a few kept free so that the
-    // chain's potrf / trsm / strip launches never wait for a whole update.
+    // chain's launches never wait for a whole update.
     const int32_t rest_ctas = std::max(16, ctx->num_sms - ctx->grad_sms - 8);
     {
         const int64_t nrest = nb > 2 ? nb - 2 : 0;
         int sub_h = 0;  // inverse levels of the first half (stream4, below)
         for (int32_t m = kT; m < Vp / 2; m *= 2) sub_h++;
-        KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + 3 * (int64_t)(nb - 1) + nrest +
+        KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + 3 * (int64_t)(nb - 1) + 3 * nrest +
                                                      (nb > 1 ? 2 + 3 * (int64_t)sub_h : 0));
         jacobi_kernel<<<nblk(Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, ctx->mx_dinv.as<double>());
         scale_to_f32_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, S);
         TPE_CUDA_TRY(cudaGetLastError());
-        int last_rest = -1;
         for (int j = 0; j < nb; j++) {
             const int32_t j0 = j * kT;
             potrf128_kernel<<<1, 256, potrf_smem, st>>>(S, Vp, j0, mf.Z.hi, mf.Z.lo, d_bad);
             TPE_CUDA_TRY(cudaGetLastError());
             if (j + 1 == nb) break;
             const int32_t rows = Vp - j0 - kT;
+            const bool more = rows > kT;  // rows below block j+1 (then also a trailing update)
+            // block column j below its diagonal is final once the previous
+            // step's column update has run (which itself followed the trailing
+            // update before it)
+            if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_s[j - 1], 0));
             split_copy_kernel<<<nblk((int64_t)rows * kT, 256), 256, 0, st>>>(
                 S, Vp, j0 + kT, j0, rows, mf.L.hi, mf.L.lo);
             TPE_CUDA_TRY(cudaGetLastError());
-            tc::GemmArgs t;  // L21 = S21 Z_jj^T (in place in L)
+            tc::GemmArgs t;  // L_{j+1,j} = S_{j+1,j} Z_jj^T (in place in L)
             t.a_r0 = j0 + kT;
             t.a_c0 = j0;
             t.b_r0 = j0;
             t.b_c0 = j0;
             t.c_r0 = j0 + kT;
             t.c_c0 = j0;
-            t.M = rows;
+            t.M = kT;
             t.N = kT;
             t.K = kT;
             TC_TRY(tc::gemm_nt(mf.L, mf.Z, mf.L, t, d_err, st));
+            TPE_CUDA_TRY(cudaEventRecord(ev_t1[j], st));
+            if (more) {
+                TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_t1[j], 0));
+                tc::GemmArgs t2 = t;  // the rest of the panel: rows j0+256 ..
+                t2.a_r0 = t2.c_r0 = j0 + 2 * kT;
+                t2.M = rows - kT;
+                TC_TRY(tc::gemm_nt(mf.L, mf.Z, mf.L, t2, d_err, st5));
+                TPE_CUDA_TRY(cudaEventRecord(ev_tr[j], st5));
+                // trailing update (low priority): S[j0+256.., j0+256..] -= L21 L21^T, lower tiles
+                TPE_CUDA_TRY(cudaStreamWaitEvent(st2, ev_tr[j], 0));
+                tc::GemmArgs u;
+                u.a_r0 = u.b_r0 = j0 + 2 * kT;
+                u.a_c0 = u.b_c0 = j0;
+                u.c_r0 = u.c_c0 = j0 + 2 * kT;
+                u.M = u.N = rows - kT;
+                u.K = kT;
+                u.mode = tc::kLowerTiles;
+                u.alpha = -1.0f;
+                u.beta = 1.0f;
+                // block column j+1 below block j+1: after the previous trailing update
+                if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_r[j - 1], 0));
+                tc::GemmArgs v;  // S[j0+256.., block j+1] -= L_{rows,j} L_{j+1,j}^T
+                v.a_r0 = j0 + 2 * kT;
+                v.a_c0 = j0;
+                v.b_r0 = j0 + kT;
+                v.b_c0 = j0;
+                v.c_r0 = j0 + 2 * kT;
+                v.c_c0 = j0 + kT;
+                v.M = rows - kT;
+                v.N = kT;
+                v.K = kT;
+                v.alpha = -1.0f;
+                v.beta = 1.0f;
+                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, v, d_err, st5));
+                TPE_CUDA_TRY(cudaEventRecord(ev_s[j], st5));
+                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2, rest_ctas, d_ctr + j));
+                TPE_CUDA_TRY(cudaEventRecord(ev_r[j], st2));
+            }
             if (nb > 1 && j == nb / 2 - 1) {
                 // panels 0 .. nb/2-1 are final: the first half of the inverse and
                 // the top level's T^T = W11 L21^T go to stream4 (low priority)
-                TPE_CUDA_TRY(cudaEventRecord(ev_mid, st));
+                TPE_CUDA_TRY(cudaEventRecord(ev_mid, more ? st5 : st));
                 TPE_CUDA_TRY(cudaStreamWaitEvent(ctx->stream4, ev_mid, 0));
                 const int32_t H = Vp / 2;
                 TPE_TRY(inverse_half(ctx, 0, H, ctx->stream4, d_err, d_ctr + Vp / kT));
@@ -845,39 +893,23 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
                 TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T2, t2, d_err, ctx->stream4));
                 TPE_CUDA_TRY(cudaEventRecord(ev_half, ctx->stream4));
             }
-            if (rows > kT) {
-                // rest: S[j0+256.., j0+256..] -= L21 L21^T on lower tiles (low priority stream)
-                TPE_CUDA_TRY(cudaEventRecord(ev_t[j], st));
-                TPE_CUDA_TRY(cudaStreamWaitEvent(st2, ev_t[j], 0));
-                tc::GemmArgs u;
-                u.a_r0 = u.b_r0 = j0 + 2 * kT;
-                u.a_c0 = u.b_c0 = j0;
-                u.c_r0 = u.c_c0 = j0 + 2 * kT;
-                u.M = u.N = rows - kT;
-                u.K = kT;
-                u.mode = tc::kLowerTiles;
-                u.alpha = -1.0f;
-                u.beta = 1.0f;
-                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2, rest_ctas, d_ctr + j));
-                TPE_CUDA_TRY(cudaEventRecord(ev_r[j], st2));
-            }
-            if (last_rest >= 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[last_rest], 0));
-            if (rows > kT) last_rest = j;
-            tc::GemmArgs v;  // strip: block column j+1 (rows j0+128..) -= L21 L21[0:128]^T
-            v.a_r0 = j0 + kT;
-            v.a_c0 = j0;
-            v.b_r0 = j0 + kT;
-            v.b_c0 = j0;
-            v.c_r0 = j0 + kT;
-            v.c_c0 = j0 + kT;
-            v.M = rows;
-            v.N = kT;
-            v.K = kT;
-            v.alpha = -1.0f;
-            v.beta = 1.0f;
-            TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, v, d_err, st));
+            // the next diagonal block: after the previous trailing update, which
+            // also reaches it
+            if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[j - 1], 0));
+            tc::GemmArgs w;  // S_{j+1,j+1} -= L_{j+1,j} L_{j+1,j}^T
+            w.a_r0 = w.b_r0 = j0 + kT;
+            w.a_c0 = w.b_c0 = j0;
+            w.c_r0 = w.c_c0 = j0 + kT;
+            w.M = w.N = w.K = kT;
+            w.alpha = -1.0f;
+            w.beta = 1.0f;
+            TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, w, d_err, st));
         }
-        if (last_rest >= 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[last_rest], 0));
+        // the whole factor (every panel solved, every update applied) before the inverse
+        TPE_CUDA_TRY(cudaEventRecord(ev_side, st5));
+        TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_side, 0));
+        TPE_CUDA_TRY(cudaEventRecord(ev_side, st2));
+        TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_side, 0));
     }
     {
         // Z = L^{-1} (W = Z^T alongside) by recursive halving. The first half

@@ -103,6 +103,7 @@ struct tpe_ctx {
     cudaStream_t stream2 = nullptr;           // look-ahead stream of the factorization
     cudaStream_t stream3 = nullptr;           // the gradient, concurrent with assembly + factor
     cudaStream_t stream4 = nullptr;           // first half of the mixed inverse, beside the factor
+    cudaStream_t stream5 = nullptr;           // panel remainders of the mixed factor (high priority)
     cudaEvent_t ev_prep = nullptr, ev_grad = nullptr;
     // a gradient launched on stream3 and not yet joined (step_impl / finish_gradient)
     bool grad_pending = false;
