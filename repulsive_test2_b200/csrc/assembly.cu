@@ -189,7 +189,7 @@ __global__ void pair_diag_kernel(const double4* __restrict__ ea, int32_t E, int3
 // A[v][u] = sum_{(I,a) in inc(v)} sum_{(J,b) in inc(u)} (s_a s_b Mb'[I][J] + M0'[I][J]),
 // s_0 = +1 (v is the edge's first vertex), s_1 = -1. Lower-triangle tiles only;
 // each entry is written with its mirror.
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(1024, 2)
 gather_A_kernel(const double2* __restrict__ M, int32_t E, const int32_t* __restrict__ inc_off,
                 const int32_t* __restrict__ inc, int32_t V, int32_t tiles, double* __restrict__ A,
                 double* __restrict__ B, double* __restrict__ B0) {
@@ -197,6 +197,13 @@ gather_A_kernel(const double2* __restrict__ M, int32_t E, const int32_t* __restr
     // written along rows, and its mirror (tj, ti) through a shared-memory
     // transpose, so both stores are coalesced.
     __shared__ double ta[32][33], tb[32][33], t0[32][33];
+    // the incidence lists of the tile's 32 rows and 32 columns, staged once
+    // (vertices of degree <= kDeg; a tile with a larger degree reads them from
+    // global memory as it goes)
+    constexpr int kDeg = 4;
+    __shared__ int32_t inc_r[32][kDeg], inc_c[32][kDeg];
+    __shared__ int32_t deg_r[32], deg_c[32];
+    __shared__ int big;
     const int32_t t = blockIdx.x;
     int32_t ti = (int32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
     while ((int64_t)ti * (ti + 1) / 2 > t) ti--;
@@ -207,8 +214,41 @@ gather_A_kernel(const double2* __restrict__ M, int32_t E, const int32_t* __restr
     const int32_t u = tj * 32 + tx;
     (void)tiles;
     const bool ok = v < V && u < V && u <= v;
+    const int tid = ty * 32 + tx;
+    if (tid == 0) big = 0;
+    __syncthreads();
+    if (tid < 64) {
+        const int k = tid & 31;
+        const bool isrow = tid < 32;
+        const int32_t w = (isrow ? ti : tj) * 32 + k;
+        int32_t n = 0;
+        if (w < V) {
+            const int32_t b = inc_off[w];
+            n = inc_off[w + 1] - b;
+            if (n > kDeg) big = 1;
+            for (int q = 0; q < n && q < kDeg; q++) (isrow ? inc_r : inc_c)[k][q] = inc[b + q];
+        }
+        (isrow ? deg_r : deg_c)[k] = n;
+    }
+    __syncthreads();
     double sb = 0.0, s0 = 0.0;
-    if (ok) {
+    if (ok && !big) {
+        // same sums, same order as below
+        for (int p = 0; p < deg_r[ty]; p++) {
+            const int32_t ip = inc_r[ty][p];
+            const int32_t I = ip >> 1;
+            const double sa = (ip & 1) ? -1.0 : 1.0;
+            const double2* row = M + (int64_t)I * E;
+            for (int q = 0; q < deg_c[tx]; q++) {
+                const int32_t iq = inc_c[tx][q];
+                const int32_t J = iq >> 1;
+                const double sgn = (iq & 1) ? -sa : sa;
+                const double2 m = row[J];
+                sb += sgn * m.x;
+                s0 += m.y;
+            }
+        }
+    } else if (ok) {
         for (int32_t p = inc_off[v]; p < inc_off[v + 1]; p++) {
             const int32_t I = inc[p] >> 1;
             const double sa = (inc[p] & 1) ? -1.0 : 1.0;
