@@ -72,3 +72,13 @@ def test_per_edge_2048_properties():
     assert np.linalg.norm(ell1 - ell) <= 1e-10 * max(1.0, float(np.sum(ell)))
     assert rmx["stats"]["tau"] == r64["stats"]["tau"]
     assert np.array_equal(rmx["vertices"], r64["vertices"])
+
+
+def test_per_edge_repeated_steps_are_bit_identical():
+    v, e = F.random_walk_knot(512, seed=12)
+    blocks = _per_edge(v, e)
+    o = {"projectionMode": "frozen", "trials": 8, "collectField": True}
+    runs = [T.sobolevStepSet(v, e, None, blocks, o) for _ in range(2)]
+    assert runs[1]["energy"] == runs[0]["energy"]
+    assert np.array_equal(runs[1]["vertices"], runs[0]["vertices"])
+    assert np.array_equal(runs[1]["descentField"], runs[0]["descentField"])
