@@ -485,13 +485,14 @@ mrhs_dmma_kernel(const MT* __restrict__ M, int32_t ldm, int32_t n,
             xs[jj * kXs + c] = (c < nr && jj < kn) ? X[(size_t)c * ldx + kc + jj] : 0.0;
         }
         __syncthreads();
-        // four 16-column groups per pass: their loads of M are all issued before
-        // the first MMA (the MMA order, and so the sums, are those of one group
-        // at a time)
-        for (int g0 = 0; g0 < kn; g0 += 64) {
-            double a[4][4];
+        // kUG 16-column groups per pass (the same bytes in flight per thread for
+        // FP32 and FP64 M): their loads of M are all issued before the first MMA
+        // (the MMA order, and so the sums, are those of one group at a time)
+        constexpr int kUG = sizeof(MT) == 8 ? 4 : 8;
+        for (int g0 = 0; g0 < kn; g0 += 16 * kUG) {
+            MT a[kUG][4];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < kUG; u++) {
                 const int32_t col = kc + g0 + 16 * u + m4;
                 if (g0 + 16 * u < kn && rin && vec && col + 3 < ke) {
                     if constexpr (sizeof(MT) == 8) {
@@ -511,18 +512,18 @@ mrhs_dmma_kernel(const MT* __restrict__ M, int32_t ldm, int32_t n,
                 } else {
 #pragma unroll
                     for (int t = 0; t < 4; t++)
-                        a[u][t] = (g0 + 16 * u < kn && rin && col + t < ke) ? (double)mrow[col + t] : 0.0;
+                        a[u][t] = (g0 + 16 * u < kn && rin && col + t < ke) ? mrow[col + t] : (MT)0;
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < kUG; u++) {
                 const int g = g0 + 16 * u;
                 if (g >= kn) break;
 #pragma unroll
                 for (int s4 = 0; s4 < 4; s4++) {
                     const double* xr = xs + (g + m4 + s4) * kXs;
-                    dmma884(c0a, c0b, a[u][s4], xr[gq]);
-                    dmma884(c1a, c1b, a[u][s4], xr[8 + gq]);
+                    dmma884(c0a, c0b, (double)a[u][s4], xr[gq]);
+                    dmma884(c1a, c1b, (double)a[u][s4], xr[8 + gq]);
                 }
             }
         }
