@@ -557,15 +557,31 @@ __global__ void mrhs_reduce_kernel(const double* __restrict__ part, int32_t nspl
 // Plain FP32 copies of the inverse factor (hi + lo is exact in FP32): Zf = Z on
 // lower tiles (diagonal tiles included, their upper parts are zero), Wf = W
 // on upper tiles. The CG applies them with FP64 arithmetic.
+// Restricted to the diagonal block [r0, r0 + n)^2 (the top level's
+// off-diagonal blocks are written in FP32 directly).
 __global__ void factor_to_f32_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
                                      const float* __restrict__ whi, const float* __restrict__ wlo,
-                                     int32_t Vp, float* __restrict__ zf, float* __restrict__ wf) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int64_t)Vp * Vp) return;
-    const int32_t i = (int32_t)(t / Vp), j = (int32_t)(t % Vp);
+                                     int32_t Vp, int32_t r0, int32_t n, float* __restrict__ zf,
+                                     float* __restrict__ wf) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n * n) return;
+    const int32_t i = r0 + (int32_t)(e / n), j = r0 + (int32_t)(e % n);
+    const int64_t t = (int64_t)i * Vp + j;
     const int ti = i / kT, tj = j / kT;
     if (ti >= tj) zf[t] = zhi[t] + zlo[t];
     if (ti <= tj) wf[t] = whi[t] + wlo[t];
+}
+
+// Wf[c][base + r] = Zf[base + r][c] (r, c < m): the top level's W12 = Z21^T in FP32.
+__global__ void transpose_f32_kernel(const float* __restrict__ zf, float* __restrict__ wf,
+                                     int32_t ld, int32_t m, int32_t base) {
+    __shared__ float t[32][33];
+    const int32_t r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y)
+        t[yy][threadIdx.x] = zf[(size_t)(base + r0 + yy) * ld + c0 + threadIdx.x];
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y)
+        wf[(size_t)(c0 + yy) * ld + base + r0 + threadIdx.x] = t[threadIdx.x][yy];
 }
 
 constexpr int kDotChunks = 32;
@@ -756,6 +772,17 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     }
     TPE_TRY(ensure(ctx, ctx->mx_Zd, sizeof(float) * (size_t)Vp * Vp));
     TPE_TRY(ensure(ctx, ctx->mx_Wd, sizeof(float) * (size_t)Vp * Vp));
+    tc::SplitMat& Zf = mf.Zf;  // the CG's FP32 copy of Z, as a plain GEMM output
+    if (Zf.hi != ctx->mx_Zd.as<float>() || Zf.rows != Vp) {
+        Zf.hi = ctx->mx_Zd.as<float>();
+        Zf.lo = nullptr;
+        Zf.rows = Zf.cols = Zf.ld = Vp;
+        if (!tc::make_maps(Zf)) {
+            Zf.hi = nullptr;
+            set_error(ctx, TPE_ERR_CUDA, "cuTensorMapEncodeTiled failed for the FP32 inverse factor");
+            return TPE_ERR_CUDA;
+        }
+    }
     TPE_TRY(ensure(ctx, ctx->status, sizeof(int32_t) * 4));
     int32_t* d_bad = ctx->status.as<int32_t>() + 2;
     TPE_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 2 * sizeof(int32_t), st));
@@ -935,17 +962,22 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             u.M = u.N = u.K = H;
             u.mode = tc::kALower;
             u.alpha = -1.0f;
-            TC_TRY(tc::gemm_nt(mf.Z, mf.T2, mf.Z, u, d_err, st, H >= 1024 ? ctx->num_sms : 0,
+            // no later product reads it split: written straight into the CG's FP32 copy
+            TC_TRY(tc::gemm_nt(mf.Z, mf.T2, mf.Zf, u, d_err, st, H >= 1024 ? ctx->num_sms : 0,
                                d_ctr + Vp / kT + 63));
-            transpose_block_kernel<<<dim3(H / 32, H / 32, 1), dim3(32, 8), 0, st>>>(
-                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, H, 0);
+            transpose_f32_kernel<<<dim3(H / 32, H / 32, 1), dim3(32, 8), 0, st>>>(
+                ctx->mx_Zd.as<float>(), ctx->mx_Wd.as<float>(), Vp, H, H);
             TPE_CUDA_TRY(cudaGetLastError());
         }
     }
     {
-        KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
-        factor_to_f32_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(
-            mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, ctx->mx_Zd.as<float>(), ctx->mx_Wd.as<float>());
+        // the diagonal halves (the whole matrix when it is one block)
+        const int32_t nh = Vp > kT ? Vp / 2 : Vp;
+        KernelScope ks(ctx, TPE_KGROUP_TRSV, Vp / nh);
+        for (int32_t r0 = 0; r0 < Vp; r0 += nh)
+            factor_to_f32_kernel<<<nblk((int64_t)nh * nh, 256), 256, 0, st>>>(
+                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, r0, nh, ctx->mx_Zd.as<float>(),
+                ctx->mx_Wd.as<float>());
         TPE_CUDA_TRY(cudaGetLastError());
     }
     int32_t flags[2] = {0, 0};

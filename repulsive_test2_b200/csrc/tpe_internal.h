@@ -82,6 +82,7 @@ struct MixedFactor {
     int V = 0, Vp = 0;
     double rho = 0.0;
     tc::SplitMat L, Z, W, T, T2;  // T: level scratch; T2: the top level's T^T
+    tc::SplitMat Zf;              // plain FP32 view of the CG's copy of Z
     tc::SplitMat S;  // plain FP32 trailing matrix (hi only)
 };
 
