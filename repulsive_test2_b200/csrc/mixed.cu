@@ -818,7 +818,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     // stream2 (low priority) the trailing update of everything to the right.
     // Every tile receives its updates in the order of the one-stream schedule
     // (rests of earlier panels first), so the results do not depend on it.
-    while ((int32_t)ctx->fac_events.size() < 4 * nb + 3) {
+    while ((int32_t)ctx->fac_events.size() < 5 * nb + 3) {
         cudaEvent_t e;
         TPE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->fac_events.push_back(e);
@@ -830,6 +830,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     cudaEvent_t ev_mid = ctx->fac_events[4 * nb];         // panels 0 .. nb/2-1 done
     cudaEvent_t ev_half = ctx->fac_events[4 * nb + 1];    // first half of the inverse done
     cudaEvent_t ev_side = ctx->fac_events[4 * nb + 2];    // side streams drained
+    cudaEvent_t* ev_sp = ctx->fac_events.data() + 4 * nb + 3;  // panel j split
     const cudaStream_t st2 = ctx->stream2, st5 = ctx->stream5;
     // The trailing updates run persistent (one CTA per SM walking its tiles) on
     // the SMs left by the concurrent gradient, minus a few kept free so that the
@@ -858,20 +859,21 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             split_copy_kernel<<<nblk((int64_t)rows * kT, 256), 256, 0, st>>>(
                 S, Vp, j0 + kT, j0, rows, mf.L.hi, mf.L.lo);
             TPE_CUDA_TRY(cudaGetLastError());
-            tc::GemmArgs t;  // L_{j+1,j} = S_{j+1,j} Z_jj^T (in place in L)
-            t.a_r0 = j0 + kT;
+            TPE_CUDA_TRY(cudaEventRecord(ev_sp[j], st));
+            // L_{j+1,j} = S_{j+1,j} Z_jj^T and the next diagonal block's update by it,
+            // one CTA; the diagonal block also gets the previous trailing update
+            if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[j - 1], 0));
+            TC_TRY(tc::chain_tile(mf.L, mf.Z, Sm, j0, d_err, st));
+            TPE_CUDA_TRY(cudaEventRecord(ev_t1[j], st));
+            tc::GemmArgs t;  // the panel below block j+1: L = S Z_jj^T (in place in L)
             t.a_c0 = j0;
             t.b_r0 = j0;
             t.b_c0 = j0;
-            t.c_r0 = j0 + kT;
             t.c_c0 = j0;
-            t.M = kT;
             t.N = kT;
             t.K = kT;
-            TC_TRY(tc::gemm_nt(mf.L, mf.Z, mf.L, t, d_err, st));
-            TPE_CUDA_TRY(cudaEventRecord(ev_t1[j], st));
             if (more) {
-                TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_t1[j], 0));
+                TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_sp[j], 0));
                 tc::GemmArgs t2 = t;  // the rest of the panel: rows j0+256 ..
                 t2.a_r0 = t2.c_r0 = j0 + 2 * kT;
                 t2.M = rows - kT;
@@ -888,7 +890,9 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
                 u.mode = tc::kLowerTiles;
                 u.alpha = -1.0f;
                 u.beta = 1.0f;
-                // block column j+1 below block j+1: after the previous trailing update
+                // block column j+1 below block j+1: after the previous trailing
+                // update, with L_{j+1,j} from the main stream
+                TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_t1[j], 0));
                 if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_r[j - 1], 0));
                 tc::GemmArgs v;  // S[j0+256.., block j+1] -= L_{rows,j} L_{j+1,j}^T
                 v.a_r0 = j0 + 2 * kT;
@@ -921,17 +925,6 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
                 TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T2, t2, d_err, ctx->stream4));
                 TPE_CUDA_TRY(cudaEventRecord(ev_half, ctx->stream4));
             }
-            // the next diagonal block: after the previous trailing update, which
-            // also reaches it
-            if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[j - 1], 0));
-            tc::GemmArgs w;  // S_{j+1,j+1} -= L_{j+1,j} L_{j+1,j}^T
-            w.a_r0 = w.b_r0 = j0 + kT;
-            w.a_c0 = w.b_c0 = j0;
-            w.c_r0 = w.c_c0 = j0 + kT;
-            w.M = w.N = w.K = kT;
-            w.alpha = -1.0f;
-            w.beta = 1.0f;
-            TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, w, d_err, st));
         }
         // the whole factor (every panel solved, every update applied) before the inverse
         TPE_CUDA_TRY(cudaEventRecord(ev_side, st5));

@@ -58,6 +58,12 @@ struct GemmArgs {
 // each walking many tiles) for whole-tile TMA epilogues; tile_ctr (device, may be
 // null) is then a zeroed counter the CTAs take tiles from, else tiles go
 // round-robin.
+// For the diagonal block at row/column j0 (a multiple of 128) of a Cholesky in
+// progress: L1 = L[j0+128.., j0..] Z[j0.., j0..]^T, written in place into L
+// (split), then D[j0+128.., j0+128..] -= L1 L1^T on a plain FP32 D, by one CTA.
+cudaError_t chain_tile(const SplitMat& L, const SplitMat& Z, const SplitMat& D, int32_t j0,
+                       int32_t* err, cudaStream_t stream);
+
 cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const GemmArgs& g,
                     int32_t* err, cudaStream_t stream, int32_t max_ctas = 0,
                     int32_t* tile_ctr = nullptr);

@@ -701,6 +701,197 @@ gemm_nt_persist_kernel(const __grid_constant__ CUtensorMap a_hi,
     }
 }
 
+// ---- one-tile panel solve fused with the next diagonal update ----------------
+//
+// For diagonal block j (origin j0): L1 = S1 Z^T with S1 = L[j0+128 .., j0 ..]
+// (the split copy of the panel's first row tile), Z = Z[j0 .., j0 ..]; L1 is
+// written split into L, kept in shared memory in the MMA operand layout, and
+// D[j0+128 .., j0+128 ..] -= L1 L1^T follows as a second product on the same
+// CTA (TMA reduce-add into the plain FP32 trailing matrix). 128 threads:
+// warp 0 lane 0 loads, warp 1 lane 0 issues the MMAs, all four warps drain
+// TMEM. Each product is hi*hi + hi*lo + lo*hi (3xTF32) like gemm_nt_kernel.
+__global__ void __launch_bounds__(128, 1)
+chain_tile_kernel(const __grid_constant__ CUtensorMap l_hi, const __grid_constant__ CUtensorMap l_lo,
+                  const __grid_constant__ CUtensorMap z_hi, const __grid_constant__ CUtensorMap z_lo,
+                  const __grid_constant__ CUtensorMap d_map, int32_t j0, int32_t* err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    // full[S], empty[S], done1, done2
+    uint64_t* bars = (uint64_t*)(smem + kStages * kStageBytes);
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * kStages + 2);
+    volatile int32_t* aborted = (volatile int32_t*)(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages),
+                   done1 = smem_u32(bars + 2 * kStages), done2 = smem_u32(bars + 2 * kStages + 1);
+    constexpr int nk = kBM / kBK;  // K = 128: four stages
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kStages; st++) {
+            mbar_init(full0 + 8 * st, 1);
+            mbar_init(empty0 + 8 * st, 1);
+        }
+        mbar_init(done1, 1);
+        mbar_init(done2, 1);
+        *aborted = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(2 * kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const int32_t r1 = j0 + kBM;  // rows of L1 (and of the diagonal block it updates)
+
+    // phase 1: L1 = S1 Z^T into TMEM columns 0 .. 127
+    if (warp == 0 && lane == 0) {
+        int issued = 0;
+        for (int it = 0; it < nk; it++) {
+            const int st = it % kStages;
+            if (it >= kStages && !mbar_wait(empty0 + 8 * st, ((it / kStages) - 1) & 1, err)) {
+                *aborted = 1;
+                break;
+            }
+            if (*aborted) break;
+            const uint32_t sa = smem_u32(smem + st * kStageBytes);
+            const uint32_t fb = full0 + 8 * st;
+            mbar_expect_tx(fb, kStageBytes);
+            const int32_t k = j0 + it * kBK;
+            tma_load_2d(sa, &l_hi, fb, k, r1);
+            tma_load_2d(sa + kTileBytes, &l_lo, fb, k, r1);
+            tma_load_2d(sa + 2 * kTileBytes, &z_hi, fb, k, j0);
+            tma_load_2d(sa + 3 * kTileBytes, &z_lo, fb, k, j0);
+            issued = it + 1;
+        }
+        for (int it = issued > kStages ? issued - kStages : 0; it < issued; it++)
+            mbar_wait(full0 + 8 * (it % kStages), (it / kStages) & 1, err);
+    } else if (warp == 1 && lane == 0) {
+        bool any = false;
+        for (int it = 0; it < nk; it++) {
+            const int st = it % kStages;
+            if (!mbar_wait(full0 + 8 * st, (it / kStages) & 1, err)) {
+                *aborted = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(smem + st * kStageBytes);
+#pragma unroll
+            for (int kk = 0; kk < kBK / 8; kk++) {
+                const uint64_t ah = sw128_desc(sa + kk * 32);
+                const uint64_t al = sw128_desc(sa + kTileBytes + kk * 32);
+                const uint64_t bh = sw128_desc(sa + 2 * kTileBytes + kk * 32);
+                const uint64_t bl = sw128_desc(sa + 3 * kTileBytes + kk * 32);
+                mma_tf32(tmem, ah, bh, (it | kk) ? 1u : 0u);
+                mma_tf32(tmem, ah, bl, 1u);
+                mma_tf32(tmem, al, bh, 1u);
+            }
+            mma_commit(empty0 + 8 * st);
+            any = true;
+        }
+        if (any)
+            mma_commit(done1);
+        else
+            mbar_arrive(done1);
+    }
+    __syncwarp();
+    __syncthreads();
+    bool ok = mbar_wait(done1, 0, err);
+    ok = __syncthreads_and(ok && !*aborted) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // L1, split, into the freed ring: hi boxes at 0, lo boxes at 4 tiles (128 rows
+    // x 32 columns each, 128B-swizzled: the TMA box and the MMA operand layout)
+    const int r = warp * 32 + lane;
+    if (ok) {
+        for (int b = 0; b < 4; b++) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(32 * b), v);
+            uint8_t* row_hi = smem + b * kTileBytes + r * 128;
+            uint8_t* row_lo = smem + 4 * kTileBytes + b * kTileBytes + r * 128;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int pq = (q ^ (r & 7)) * 16;
+                float4 h, l;
+                split(v[4 * q], h.x, l.x);
+                split(v[4 * q + 1], h.y, l.y);
+                split(v[4 * q + 2], h.z, l.z);
+                split(v[4 * q + 3], h.w, l.w);
+                *reinterpret_cast<float4*>(row_hi + pq) = h;
+                *reinterpret_cast<float4*>(row_lo + pq) = l;
+            }
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok && threadIdx.x == 0) {
+        for (int b = 0; b < 4; b++) {
+            tma_store_2d(&l_hi, smem_u32(smem + b * kTileBytes), j0 + 32 * b, r1);
+            tma_store_2d(&l_lo, smem_u32(smem + 4 * kTileBytes + b * kTileBytes), j0 + 32 * b, r1);
+        }
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+    // phase 2: L1 L1^T into TMEM columns 128 .. 255, both operands the staged L1
+    if (ok && warp == 1 && lane == 0) {
+        const uint32_t d2 = tmem + (uint32_t)kTmemCols;
+        for (int b = 0; b < 4; b++) {
+            const uint32_t hb = smem_u32(smem + b * kTileBytes);
+            const uint32_t lb = smem_u32(smem + 4 * kTileBytes + b * kTileBytes);
+#pragma unroll
+            for (int kk = 0; kk < kBK / 8; kk++) {
+                const uint64_t h = sw128_desc(hb + kk * 32);
+                const uint64_t l = sw128_desc(lb + kk * 32);
+                mma_tf32(d2, h, h, (b | kk) ? 1u : 0u);
+                mma_tf32(d2, h, l, 1u);
+                mma_tf32(d2, l, h, 1u);
+            }
+        }
+        mma_commit(done2);
+    } else if (!ok && threadIdx.x == 32) {
+        mbar_arrive(done2);
+    }
+    __syncwarp();
+    bool ok2 = mbar_wait(done2, 0, err);
+    ok2 = __syncthreads_and(ok2 && ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok2) {
+        // -L1 L1^T staged after the L1 boxes, then reduce-added into D
+        uint8_t* stage = smem + 8 * kTileBytes;
+        for (int b = 0; b < 4; b++) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kTmemCols + 32 * b), v);
+            uint8_t* row = stage + b * kTileBytes + r * 128;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int pq = (q ^ (r & 7)) * 16;
+                *reinterpret_cast<float4*>(row + pq) =
+                    make_float4(-v[4 * q], -v[4 * q + 1], -v[4 * q + 2], -v[4 * q + 3]);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (ok2) {
+            for (int b = 0; b < 4; b++)
+                tma_reduce_add_2d(&d_map, smem_u32(smem + 8 * kTileBytes + b * kTileBytes),
+                                  r1 + 32 * b, r1);
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(2 * kTmemCols)
+                     : "memory");
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -738,6 +929,20 @@ bool make_maps(SplitMat& m) {
     if (!m.lo) m.map_lo = m.map_hi;
     m.maps_ok = true;
     return true;
+}
+
+cudaError_t chain_tile(const SplitMat& L, const SplitMat& Z, const SplitMat& D, int32_t j0,
+                       int32_t* err, cudaStream_t stream) {
+    if (!L.maps_ok || !Z.maps_ok || !D.maps_ok || !L.lo || !Z.lo || D.lo || j0 < 0 || (j0 % kBM) != 0 ||
+        j0 + 2 * kBM > L.rows || j0 + kBM > L.cols || j0 + kBM > Z.rows || j0 + kBM > Z.cols ||
+        j0 + 2 * kBM > D.rows || j0 + 2 * kBM > D.cols)
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(chain_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kSmemBytes);
+    if (e != cudaSuccess) return e;
+    chain_tile_kernel<<<1, 128, kSmemBytes, stream>>>(L.map_hi, L.map_lo, Z.map_hi, Z.map_lo,
+                                                     D.map_hi, j0, err);
+    return cudaGetLastError();
 }
 
 cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const GemmArgs& g,
