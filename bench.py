@@ -488,7 +488,7 @@ def run_repulsive(args):
     groups = abi.KGROUPS
     ms_g = {g: kms[i] for i, g in enumerate(groups)}
     nl = {g: kl[i] for i, g in enumerate(groups)}
-    # The gradient runs beside the factorization on a third of the SMs (its group
+    # The gradient runs beside the factorization on two fifths of the SMs (its group
     # time is the stream3 span, not a full-GPU kernel time): the roofline is taken
     # for the dominant group on the main stream, the gradient reported apart.
     dom = max((g for g in ms_g if g != "gradient" or args.precision != "mixed"), key=lambda g: ms_g[g])
@@ -534,7 +534,7 @@ def run_repulsive(args):
     roof["group_ms"] = {g: round(ms_g[g], 3) for g in groups}
     if args.precision == "mixed" and nl["gradient"] > 0:
         nsm = torch.cuda.get_device_properties(dev).multi_processor_count
-        gsm = int(os.environ.get("TPE_GRAD_SMS", nsm // 3))
+        gsm = int(os.environ.get("TPE_GRAD_SMS", nsm * 2 // 5))
         g_ach = P * 2 * 4 * 110 * max(1, nl["gradient"] // 2) / (ms_g["gradient"] * 1e-3) / 1e12
         roof["concurrent_gradient"] = {
             "sms": gsm, "achieved": g_ach, "peak_on_its_sms": fp64_peak * gsm / nsm,

@@ -1229,15 +1229,17 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
     tpe_ctx* ctx = new tpe_ctx();
     ctx->device = device;
     // The main stream carries the factorization's critical path: give it the
-    // highest priority so its small kernels are scheduled ahead of the
-    // look-ahead stream's large trailing updates.
+    // highest priority so its one-CTA kernels are dispatched ahead of everything
+    // else; stream5 (the panel rests) one step below it, the trailing updates,
+    // the gradient and the inverse's first half lowest.
     int prio_lo = 0, prio_hi = 0;
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    const int prio_side = prio_hi < prio_lo ? prio_hi + 1 : prio_hi;
     if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->stream3, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaStreamCreateWithPriority(&ctx->stream4, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&ctx->stream5, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ctx->stream5, cudaStreamNonBlocking, prio_side) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_prep, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->ev_grad, cudaEventDisableTiming) != cudaSuccess) {
         delete ctx;
@@ -1245,7 +1247,10 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
         return nullptr;
     }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
-    ctx->grad_sms = ctx->num_sms / 3;
+    // the concurrent gradient's share: the factorization and the gradient end
+    // together at V = 8192 (a sweep of 49, 53, 57, 61 SMs: 15.55, 15.08, 14.82,
+    // 14.84 ms per step), and smaller curves factor relatively faster still
+    ctx->grad_sms = ctx->num_sms * 2 / 5;
     if (const char* g = getenv("TPE_GRAD_SMS")) {
         const int n = atoi(g);
         if (n >= 0) ctx->grad_sms = n;  // 0: an ordinary grid over all SMs

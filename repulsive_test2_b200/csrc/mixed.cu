@@ -57,18 +57,37 @@ __global__ void jacobi_kernel(const double* __restrict__ A, int32_t V, int32_t V
 }
 
 // S (Vp x Vp, FP32, ld Vp) = D (A + shift) D, identity on the pad.
-__global__ void scale_to_f32_kernel(const double* __restrict__ A, int32_t V, int32_t Vp,
-                                    double shift, const double* __restrict__ d,
-                                    float* __restrict__ S) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (int64_t)Vp * Vp) return;
-    const int32_t i = (int32_t)(t / Vp), j = (int32_t)(t % Vp);
-    float v;
-    if (i < V && j < V)
-        v = (float)(d[i] * (A[(size_t)i * V + j] + shift) * d[j]);
-    else
-        v = (i == j) ? 1.0f : 0.0f;
-    S[t] = v;
+// S[i][j] = d_i (A_ij + shift) d_j rounded to FP32 for i, j < V, the identity on
+// the pad. Four consecutive columns per thread (two 16-byte loads of A when V is
+// even, one 16-byte store of S); grid (ceil(Vp / 1024), rows), rows strided.
+__global__ void __launch_bounds__(256) scale_to_f32_kernel(const double* __restrict__ A, int32_t V,
+                                                           int32_t Vp, double shift,
+                                                           const double* __restrict__ d,
+                                                           float* __restrict__ S) {
+    const int32_t j = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (j >= Vp) return;
+    for (int32_t i = blockIdx.y; i < Vp; i += gridDim.y) {
+        float o[4];
+        if (i < V && j + 3 < V && (V & 1) == 0) {
+            const double di = d[i];
+            const double2 a0 = *reinterpret_cast<const double2*>(A + (size_t)i * V + j);
+            const double2 a1 = *reinterpret_cast<const double2*>(A + (size_t)i * V + j + 2);
+            const double2 d0 = *reinterpret_cast<const double2*>(d + j);
+            const double2 d1 = *reinterpret_cast<const double2*>(d + j + 2);
+            o[0] = (float)(di * (a0.x + shift) * d0.x);
+            o[1] = (float)(di * (a0.y + shift) * d0.y);
+            o[2] = (float)(di * (a1.x + shift) * d1.x);
+            o[3] = (float)(di * (a1.y + shift) * d1.y);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int32_t jj = j + c;
+                o[c] = (i < V && jj < V) ? (float)(d[i] * (A[(size_t)i * V + jj] + shift) * d[jj])
+                                         : (i == jj ? 1.0f : 0.0f);
+            }
+        }
+        *reinterpret_cast<float4*>(S + (size_t)i * Vp + j) = make_float4(o[0], o[1], o[2], o[3]);
+    }
 }
 
 // L[r0+i][c0+j] = split(S[r0+i][c0+j]) for i < rows, j < 128 (ld shared).
@@ -810,15 +829,17 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     const size_t potrf_smem = sizeof(float) * (2 * kT * kLd + 96 * kPl + kT + 2 * kPw * kPl);
     TPE_CUDA_TRY(cudaFuncSetAttribute(potrf128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)potrf_smem));
-    // Critical path on the main stream, per block j: potrf, split copy of the
-    // panel, the panel solve of its first row tile only (L_{j+1,j}) and the
-    // update of the next diagonal block by it; then potrf j+1. Beside it, on
-    // stream5 (high priority), the rest of the panel solve and the update of the
-    // rest of block column j+1 (which the next split copy waits for), and on
-    // stream2 (low priority) the trailing update of everything to the right.
+    // Critical path on the main stream, per block j: potrf, then one CTA that
+    // solves the panel's first row tile (L_{j+1,j}) from the FP32 matrix and
+    // updates the next diagonal block by it; then potrf j+1. Beside it, on
+    // stream5 (high priority), the split copy and solve of the rest of the panel,
+    // the update of the rest of block column j+1 and of diagonal block j+2 (which
+    // the next step's one-CTA kernel waits for), and on stream2 (low priority)
+    // the rest of the trailing update, which only stream5's next column update
+    // waits for (look-ahead of one block).
     // Every tile receives its updates in the order of the one-stream schedule
     // (rests of earlier panels first), so the results do not depend on it.
-    while ((int32_t)ctx->fac_events.size() < 5 * nb + 3) {
+    while ((int32_t)ctx->fac_events.size() < 4 * nb + 3) {
         cudaEvent_t e;
         TPE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         ctx->fac_events.push_back(e);
@@ -830,7 +851,6 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     cudaEvent_t ev_mid = ctx->fac_events[4 * nb];         // panels 0 .. nb/2-1 done
     cudaEvent_t ev_half = ctx->fac_events[4 * nb + 1];    // first half of the inverse done
     cudaEvent_t ev_side = ctx->fac_events[4 * nb + 2];    // side streams drained
-    cudaEvent_t* ev_sp = ctx->fac_events.data() + 4 * nb + 3;  // panel j split
     const cudaStream_t st2 = ctx->stream2, st5 = ctx->stream5;
     // The trailing updates run persistent (one CTA per SM walking its tiles) on
     // the SMs left by the concurrent gradient, minus a few kept free so that the
@@ -840,10 +860,11 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
         const int64_t nrest = nb > 2 ? nb - 2 : 0;
         int sub_h = 0;  // inverse levels of the first half (stream4, below)
         for (int32_t m = kT; m < Vp / 2; m *= 2) sub_h++;
-        KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + 3 * (int64_t)(nb - 1) + 3 * nrest +
+        KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + (int64_t)(nb - 1) + 4 * nrest + (nrest > 0 ? nrest - 1 : 0) +
                                                      (nb > 1 ? 2 + 3 * (int64_t)sub_h : 0));
         jacobi_kernel<<<nblk(Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, ctx->mx_dinv.as<double>());
-        scale_to_f32_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, S);
+        scale_to_f32_kernel<<<dim3((unsigned)((Vp + 1023) / 1024), (unsigned)std::min(Vp, 65535)), 256, 0,
+                              st>>>(d_A, V, Vp, shift, d, S);
         TPE_CUDA_TRY(cudaGetLastError());
         for (int j = 0; j < nb; j++) {
             const int32_t j0 = j * kT;
@@ -852,17 +873,13 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             if (j + 1 == nb) break;
             const int32_t rows = Vp - j0 - kT;
             const bool more = rows > kT;  // rows below block j+1 (then also a trailing update)
-            // block column j below its diagonal is final once the previous
-            // step's column update has run (which itself followed the trailing
-            // update before it)
-            if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_s[j - 1], 0));
-            split_copy_kernel<<<nblk((int64_t)rows * kT, 256), 256, 0, st>>>(
-                S, Vp, j0 + kT, j0, rows, mf.L.hi, mf.L.lo);
-            TPE_CUDA_TRY(cudaGetLastError());
-            TPE_CUDA_TRY(cudaEventRecord(ev_sp[j], st));
             // L_{j+1,j} = S_{j+1,j} Z_jj^T and the next diagonal block's update by it,
-            // one CTA; the diagonal block also gets the previous trailing update
-            if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_r[j - 1], 0));
+            // one CTA. Block column j below its diagonal and diagonal block j+1 are
+            // final once the previous step's stream5 work has run: the column
+            // update and the diagonal tile of the trailing update, both after the
+            // trailing update before that. The previous trailing update itself
+            // (the rest) is not waited for: it has a whole step to finish.
+            if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_s[j - 1], 0));
             TC_TRY(tc::chain_tile(mf.L, mf.Z, Sm, j0, d_err, st));
             TPE_CUDA_TRY(cudaEventRecord(ev_t1[j], st));
             tc::GemmArgs t;  // the panel below block j+1: L = S Z_jj^T (in place in L)
@@ -873,13 +890,21 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
             t.N = kT;
             t.K = kT;
             if (more) {
-                TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_sp[j], 0));
-                tc::GemmArgs t2 = t;  // the rest of the panel: rows j0+256 ..
+                // the rest of the panel (rows j0+256 ..): its split copy follows the
+                // previous column update on this stream, its solve needs Z_jj. Both
+                // start after the one-CTA kernel, so that its CTA never waits for
+                // an SM behind theirs.
+                TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_t1[j], 0));
+                split_copy_kernel<<<nblk((int64_t)(rows - kT) * kT, 256), 256, 0, st5>>>(
+                    S, Vp, j0 + 2 * kT, j0, rows - kT, mf.L.hi, mf.L.lo);
+                TPE_CUDA_TRY(cudaGetLastError());
+                tc::GemmArgs t2 = t;
                 t2.a_r0 = t2.c_r0 = j0 + 2 * kT;
                 t2.M = rows - kT;
                 TC_TRY(tc::gemm_nt(mf.L, mf.Z, mf.L, t2, d_err, st5));
                 TPE_CUDA_TRY(cudaEventRecord(ev_tr[j], st5));
-                // trailing update (low priority): S[j0+256.., j0+256..] -= L21 L21^T, lower tiles
+                // trailing update (low priority): S[j0+256.., j0+256..] -= L21 L21^T,
+                // lower tiles but the first (diagonal block j+2: stream5, below)
                 TPE_CUDA_TRY(cudaStreamWaitEvent(st2, ev_tr[j], 0));
                 tc::GemmArgs u;
                 u.a_r0 = u.b_r0 = j0 + 2 * kT;
@@ -890,9 +915,9 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
                 u.mode = tc::kLowerTiles;
                 u.alpha = -1.0f;
                 u.beta = 1.0f;
+                u.tile_skip = 1;
                 // block column j+1 below block j+1: after the previous trailing
                 // update, with L_{j+1,j} from the main stream
-                TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_t1[j], 0));
                 if (j > 0) TPE_CUDA_TRY(cudaStreamWaitEvent(st5, ev_r[j - 1], 0));
                 tc::GemmArgs v;  // S[j0+256.., block j+1] -= L_{rows,j} L_{j+1,j}^T
                 v.a_r0 = j0 + 2 * kT;
@@ -907,8 +932,14 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
                 v.alpha = -1.0f;
                 v.beta = 1.0f;
                 TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, v, d_err, st5));
+                tc::GemmArgs dg = u;  // diagonal block j+2 -= L_{j+2,j} L_{j+2,j}^T
+                dg.M = dg.N = kT;
+                dg.mode = 0;
+                dg.tile_skip = 0;
+                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, dg, d_err, st5));
                 TPE_CUDA_TRY(cudaEventRecord(ev_s[j], st5));
-                TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2, rest_ctas, d_ctr + j));
+                if (rows - kT > kT)
+                    TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2, rest_ctas, d_ctr + j));
                 TPE_CUDA_TRY(cudaEventRecord(ev_r[j], st2));
             }
             if (nb > 1 && j == nb / 2 - 1) {

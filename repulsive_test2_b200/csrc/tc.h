@@ -52,6 +52,9 @@ struct GemmArgs {
     int32_t mode = 0;
     int32_t nbatch = 1;
     float alpha = 1.0f, beta = 0.0f;
+    // persistent form only: the first tile_skip output tiles in tile order
+    // (packed lower tiles with kLowerTiles, else row-major, batch last) are left out
+    int32_t tile_skip = 0;
 };
 
 // max_ctas > 0 selects the persistent form (at most max_ctas CTAs, one per SM,
@@ -59,8 +62,8 @@ struct GemmArgs {
 // null) is then a zeroed counter the CTAs take tiles from, else tiles go
 // round-robin.
 // For the diagonal block at row/column j0 (a multiple of 128) of a Cholesky in
-// progress: L1 = L[j0+128.., j0..] Z[j0.., j0..]^T, written in place into L
-// (split), then D[j0+128.., j0+128..] -= L1 L1^T on a plain FP32 D, by one CTA.
+// progress on a plain FP32 D: L1 = D[j0+128.., j0..] Z[j0.., j0..]^T, written
+// split into L, then D[j0+128.., j0+128..] -= L1 L1^T, by one CTA.
 cudaError_t chain_tile(const SplitMat& L, const SplitMat& Z, const SplitMat& D, int32_t j0,
                        int32_t* err, cudaStream_t stream);
 

@@ -506,7 +506,8 @@ gemm_nt_persist_kernel(const __grid_constant__ CUtensorMap a_hi,
         if (lane == 0) {
             int it = 0;  // ring slots used so far
             for (int i = 0;; i++) {
-                int x = tile_ctr ? atomicAdd(tile_ctr, 1) : (int)blockIdx.x + i * (int)gridDim.x;
+                int x = (tile_ctr ? atomicAdd(tile_ctr, 1) : (int)blockIdx.x + i * (int)gridDim.x) +
+                        g.tile_skip;
                 if (x >= ntiles) x = -1;
                 int z = 0, ti = 0, tj = 0, kb = 0, nk = 0;
                 if (x >= 0) {
@@ -703,31 +704,40 @@ gemm_nt_persist_kernel(const __grid_constant__ CUtensorMap a_hi,
 
 // ---- one-tile panel solve fused with the next diagonal update ----------------
 //
-// For diagonal block j (origin j0): L1 = S1 Z^T with S1 = L[j0+128 .., j0 ..]
-// (the split copy of the panel's first row tile), Z = Z[j0 .., j0 ..]; L1 is
-// written split into L, kept in shared memory in the MMA operand layout, and
+// For diagonal block j (origin j0): L1 = S1 Z^T with S1 = D[j0+128 .., j0 ..]
+// (the panel's first row tile, read from the plain FP32 trailing matrix D and
+// split in shared memory) and Z = Z[j0 .., j0 ..]; L1 is written split into L,
+// kept in shared memory in the MMA operand layout, and
 // D[j0+128 .., j0+128 ..] -= L1 L1^T follows as a second product on the same
-// CTA (TMA reduce-add into the plain FP32 trailing matrix). 128 threads:
-// warp 0 lane 0 loads, warp 1 lane 0 issues the MMAs, all four warps drain
-// TMEM. Each product is hi*hi + hi*lo + lo*hi (3xTF32) like gemm_nt_kernel.
+// CTA (TMA reduce-add into D). 128 threads: warp 0 lane 0 loads, warp 1 lane 0
+// issues the MMAs, all four warps split S1 and drain TMEM. Each product is
+// hi*hi + hi*lo + lo*hi (3xTF32) in gemm_nt_kernel's order, so the results
+// equal a split copy of S1 followed by two gemm_nt launches bit for bit.
+// Shared memory (16 KB tiles): 0-3 S1 split in place to hi, 4-7 its lo, 8-11 a
+// two-stage ring of Z (hi, lo) boxes; later L1 (hi 0-3, lo 4-7) and the staged
+// update (8-11).
 __global__ void __launch_bounds__(128, 1)
 chain_tile_kernel(const __grid_constant__ CUtensorMap l_hi, const __grid_constant__ CUtensorMap l_lo,
                   const __grid_constant__ CUtensorMap z_hi, const __grid_constant__ CUtensorMap z_lo,
                   const __grid_constant__ CUtensorMap d_map, int32_t j0, int32_t* err) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    // full[S], empty[S], done1, done2
-    uint64_t* bars = (uint64_t*)(smem + kStages * kStageBytes);
-    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * kStages + 2);
+    constexpr int kZS = 2;  // Z ring stages
+    // sfull, zfull[2], zempty[2], done1, done2
+    uint64_t* bars = (uint64_t*)(smem + 12 * kTileBytes);
+    uint32_t* tmem_slot = (uint32_t*)(bars + 8);
     volatile int32_t* aborted = (volatile int32_t*)(tmem_slot + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + kStages),
-                   done1 = smem_u32(bars + 2 * kStages), done2 = smem_u32(bars + 2 * kStages + 1);
-    constexpr int nk = kBM / kBK;  // K = 128: four stages
+    const uint32_t sfull = smem_u32(bars), zfull0 = smem_u32(bars + 1),
+                   zempty0 = smem_u32(bars + 1 + kZS), done1 = smem_u32(bars + 1 + 2 * kZS),
+                   done2 = smem_u32(bars + 2 + 2 * kZS);
+    constexpr int nk = kBM / kBK;  // K = 128: four boxes of 32 columns
+    const int32_t r1 = j0 + kBM;   // rows of L1 (and of the diagonal block it updates)
     if (threadIdx.x == 0) {
-        for (int st = 0; st < kStages; st++) {
-            mbar_init(full0 + 8 * st, 1);
-            mbar_init(empty0 + 8 * st, 1);
+        mbar_init(sfull, 1);
+        for (int st = 0; st < kZS; st++) {
+            mbar_init(zfull0 + 8 * st, 1);
+            mbar_init(zempty0 + 8 * st, 1);
         }
         mbar_init(done1, 1);
         mbar_init(done2, 1);
@@ -745,51 +755,78 @@ chain_tile_kernel(const __grid_constant__ CUtensorMap l_hi, const __grid_constan
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    const int32_t r1 = j0 + kBM;  // rows of L1 (and of the diagonal block it updates)
+    auto load_z = [&](int it) {
+        const int st = it % kZS;
+        const uint32_t fb = zfull0 + 8 * st;
+        const uint32_t dz = smem_u32(smem + (8 + 2 * st) * kTileBytes);
+        mbar_expect_tx(fb, 2 * kTileBytes);
+        tma_load_2d(dz, &z_hi, fb, j0 + it * kBK, j0);
+        tma_load_2d(dz + kTileBytes, &z_lo, fb, j0 + it * kBK, j0);
+    };
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(sfull, 4 * kTileBytes);
+        for (int b = 0; b < nk; b++)
+            tma_load_2d(smem_u32(smem + b * kTileBytes), &d_map, sfull, j0 + b * kBK, r1);
+        for (int it = 0; it < kZS; it++) load_z(it);
+    }
+    // S1 -> (hi in place, lo four tiles on); elementwise, so the swizzle carries over
+    bool ok = mbar_wait(sfull, 0, err);
+    ok = __syncthreads_and(ok) != 0;
+    if (ok) {
+        for (int i = threadIdx.x; i < nk * kTileBytes / 16; i += blockDim.x) {
+            float4* ph = reinterpret_cast<float4*>(smem) + i;
+            float4 x = *ph, h, l;
+            split(x.x, h.x, l.x);
+            split(x.y, h.y, l.y);
+            split(x.z, h.z, l.z);
+            split(x.w, h.w, l.w);
+            *ph = h;
+            *reinterpret_cast<float4*>(smem + nk * kTileBytes + 16 * i) = l;
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
 
     // phase 1: L1 = S1 Z^T into TMEM columns 0 .. 127
-    if (warp == 0 && lane == 0) {
-        int issued = 0;
-        for (int it = 0; it < nk; it++) {
-            const int st = it % kStages;
-            if (it >= kStages && !mbar_wait(empty0 + 8 * st, ((it / kStages) - 1) & 1, err)) {
-                *aborted = 1;
-                break;
+    if (threadIdx.x == 0) {
+        int issued = kZS;
+        if (ok) {
+            for (int it = kZS; it < nk; it++) {
+                const int st = it % kZS;
+                if (!mbar_wait(zempty0 + 8 * st, ((it / kZS) - 1) & 1, err)) {
+                    *aborted = 1;
+                    break;
+                }
+                if (*aborted) break;
+                load_z(it);
+                issued = it + 1;
             }
-            if (*aborted) break;
-            const uint32_t sa = smem_u32(smem + st * kStageBytes);
-            const uint32_t fb = full0 + 8 * st;
-            mbar_expect_tx(fb, kStageBytes);
-            const int32_t k = j0 + it * kBK;
-            tma_load_2d(sa, &l_hi, fb, k, r1);
-            tma_load_2d(sa + kTileBytes, &l_lo, fb, k, r1);
-            tma_load_2d(sa + 2 * kTileBytes, &z_hi, fb, k, j0);
-            tma_load_2d(sa + 3 * kTileBytes, &z_lo, fb, k, j0);
-            issued = it + 1;
         }
-        for (int it = issued > kStages ? issued - kStages : 0; it < issued; it++)
-            mbar_wait(full0 + 8 * (it % kStages), (it / kStages) & 1, err);
+        for (int it = issued - kZS; it < issued; it++)
+            mbar_wait(zfull0 + 8 * (it % kZS), (it / kZS) & 1, err);
     } else if (warp == 1 && lane == 0) {
         bool any = false;
-        for (int it = 0; it < nk; it++) {
-            const int st = it % kStages;
-            if (!mbar_wait(full0 + 8 * st, (it / kStages) & 1, err)) {
+        for (int it = 0; ok && it < nk; it++) {
+            const int st = it % kZS;
+            if (!mbar_wait(zfull0 + 8 * st, (it / kZS) & 1, err)) {
                 *aborted = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = smem_u32(smem + st * kStageBytes);
+            const uint32_t sh = smem_u32(smem + it * kTileBytes);
+            const uint32_t sl = smem_u32(smem + (nk + it) * kTileBytes);
+            const uint32_t zh = smem_u32(smem + (8 + 2 * st) * kTileBytes);
 #pragma unroll
             for (int kk = 0; kk < kBK / 8; kk++) {
-                const uint64_t ah = sw128_desc(sa + kk * 32);
-                const uint64_t al = sw128_desc(sa + kTileBytes + kk * 32);
-                const uint64_t bh = sw128_desc(sa + 2 * kTileBytes + kk * 32);
-                const uint64_t bl = sw128_desc(sa + 3 * kTileBytes + kk * 32);
+                const uint64_t ah = sw128_desc(sh + kk * 32);
+                const uint64_t al = sw128_desc(sl + kk * 32);
+                const uint64_t bh = sw128_desc(zh + kk * 32);
+                const uint64_t bl = sw128_desc(zh + kTileBytes + kk * 32);
                 mma_tf32(tmem, ah, bh, (it | kk) ? 1u : 0u);
                 mma_tf32(tmem, ah, bl, 1u);
                 mma_tf32(tmem, al, bh, 1u);
             }
-            mma_commit(empty0 + 8 * st);
+            mma_commit(zempty0 + 8 * st);
             any = true;
         }
         if (any)
@@ -799,7 +836,7 @@ chain_tile_kernel(const __grid_constant__ CUtensorMap l_hi, const __grid_constan
     }
     __syncwarp();
     __syncthreads();
-    bool ok = mbar_wait(done1, 0, err);
+    ok = mbar_wait(done1, 0, err) && ok;
     ok = __syncthreads_and(ok && !*aborted) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // L1, split, into the freed ring: hi boxes at 0, lo boxes at 4 tiles (128 rows
@@ -986,11 +1023,14 @@ cudaError_t gemm_nt(const SplitMat& A, const SplitMat& B, SplitMat& C, const Gem
             P.tma_epi = 2;
     }
     const int64_t ntiles = (int64_t)grid.x * grid.y * grid.z;
-    if (max_ctas > 0 && P.tma_epi != 0 && ntiles > 1 && ntiles < (1LL << 30)) {
+    const bool persist = max_ctas > 0 && P.tma_epi != 0 && ntiles > 1 && ntiles < (1LL << 30);
+    if (g.tile_skip != 0 && (!persist || g.tile_skip < 0 || g.tile_skip >= ntiles))
+        return cudaErrorInvalidValue;
+    if (persist) {
         e = cudaFuncSetAttribute(gemm_nt_persist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kPSmemBytes);
         if (e != cudaSuccess) return e;
-        const unsigned nb = (unsigned)std::min<int64_t>(ntiles, max_ctas);
+        const unsigned nb = (unsigned)std::min<int64_t>(ntiles - g.tile_skip, max_ctas);
         gemm_nt_persist_kernel<<<nb, kPThreads, kPSmemBytes, stream>>>(
             A.map_hi, A.map_lo, B.map_hi, B.map_lo, C.map_hi, C.map_lo, P, tm, tn, (int32_t)ntiles,
             tile_ctr);
