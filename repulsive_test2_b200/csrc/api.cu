@@ -361,7 +361,7 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
     op.mixed = false;
     op.mixed_fallback = false;
     op.refine_iters = 0;
-    op.refine_max_iter = o ? o->refine_max_iter : 30;
+    op.refine_max_iter = o ? o->refine_max_iter : 60;
     op.refine_tol = o ? o->refine_tol : 1e-12;
     op.V = V;
     op.k = k;
@@ -1206,7 +1206,7 @@ void tpe_default_step_opts(tpe_step_opts* o) {
     o->proj_max_iter = 8;
     o->precision = TPE_PRECISION_FP64;
     o->trials = 8;
-    o->refine_max_iter = 30;
+    o->refine_max_iter = 60;
     o->refine_tol = 1e-12;
 }
 

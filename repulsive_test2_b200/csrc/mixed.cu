@@ -1039,6 +1039,9 @@ int32_t mrhs_fp64(tpe_ctx* ctx, const double* M, int32_t n, const double* X, int
 // alias) by CG on the scaled system preconditioned with the FP32 inverse factor.
 // *iters = iterations of the last pass; *converged = every column reached
 // ||B - A_rho X|| <= tol ||B||.
+constexpr int kPredictFrom = 30;  // CG iterations always allowed before a predicted stop
+constexpr int kRateSpan = 10;     // iterations the residual rate is measured over
+
 int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* d_X, int32_t nr,
                     int32_t maxit, double tol, int32_t* iters, bool* converged) {
     const MixedFactor& mf = ctx->mf;
@@ -1069,6 +1072,8 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
     const float* Zf = ctx->mx_Zd.as<float>();
     const float* Wf = ctx->mx_Wd.as<float>();
     std::vector<double> hres(kMaxRhs), hbn(kMaxRhs);
+    // squared residual norms per iteration, for the predicted stop below
+    std::vector<double> hist((size_t)(maxit > 0 ? maxit + 1 : 1) * kMaxRhs);
     int32_t max_iters = 0;
     const unsigned rb_V = (unsigned)((V + kMvRows - 1) / kMvRows);
     const unsigned rb_Vp = (unsigned)(Vp / kMvRows);
@@ -1135,6 +1140,25 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
             for (int c = 0; c < n; c++)
                 if (!(hres[c] <= tol * tol * hbn[c])) done = false;
             if (done) break;
+            // From iteration kPredictFrom on, stop (not converged: the caller falls
+            // back to the FP64 factorization) once a column's residual rate over
+            // the last kRateSpan iterations predicts it reaches tol only after maxit.
+            std::copy(hres.begin(), hres.begin() + n, hist.begin() + (size_t)it * kMaxRhs);
+            if (it >= kPredictFrom && it >= kRateSpan) {
+                bool hopeless = false;
+                for (int c = 0; c < n && !hopeless; c++) {
+                    const double target = tol * tol * hbn[c];
+                    if (hres[c] <= target) continue;
+                    const double now = hres[c], old = hist[(size_t)(it - kRateSpan) * kMaxRhs + c];
+                    if (!(now < old) || !(now > 0.0)) {
+                        hopeless = true;
+                    } else {
+                        const double rate = log(now / old) / kRateSpan;  // < 0
+                        hopeless = it + log(target / now) / rate > maxit;
+                    }
+                }
+                if (hopeless) break;
+            }
             TPE_TRY(precond(R, Zv));
             TPE_TRY(dots(R, Zv, nullptr, rz[it & 1]));
             {

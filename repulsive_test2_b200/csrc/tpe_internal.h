@@ -54,7 +54,7 @@ struct SaddleOp {
     bool mixed = false;              // solves use the FP32 factor + FP64 CG (mixed.cu)
     bool mixed_fallback = false;     // mixed requested, FP64 factorization used instead
     int refine_iters = 0;            // CG iterations of the factor-time solve
-    int refine_max_iter = 30;
+    int refine_max_iter = 60;
     double refine_tol = 1e-12;
     double rho = 0.0;                // A_rho = A + (rho/V) 1 1^T
     // device (views into ctx buffers)
