@@ -34,7 +34,7 @@ enum {
     TPE_ERR_NO_TOPOLOGY = 5,      /* tpe_set_topology has not been called */
     TPE_ERR_OUT_OF_MEMORY = 6,
     TPE_ERR_INVALID_SET = 7,      /* totalLength + edgeLengths in one set (constraintSet.ts:333-344) */
-    TPE_ERR_REFINE_NOT_CONVERGED = 8, /* mixed path: FP64 refinement hit its cap */
+    TPE_ERR_REFINE_NOT_CONVERGED = 8, /* mixed path: the FP64 CG hit its cap */
     TPE_ERR_DEVICE_TIMEOUT = 9,   /* a bounded device-side wait gave up */
     TPE_ERR_TOO_LARGE = 10        /* request exceeds a fixed-capacity buffer */
 };
@@ -108,7 +108,7 @@ typedef struct {
                                       (extension; default 8, 1 = one at a time; the accepted tau
                                       and vertices do not depend on it) */
     int32_t collect_field;         /* write g~ into descent_field when non-null */
-    int32_t refine_max_iter;       /* mixed path: FP64 refinement cap (extension) */
+    int32_t refine_max_iter;       /* mixed path: CG iteration cap, default 60 (extension) */
     int32_t reserved;
     double refine_tol;             /* mixed path: relative residual target (extension) */
 } tpe_step_opts;
