@@ -716,6 +716,9 @@ gemm_nt_persist_kernel(const __grid_constant__ CUtensorMap a_hi,
 // Shared memory (16 KB tiles): 0-3 S1 split in place to hi, 4-7 its lo, 8-11 a
 // two-stage ring of Z (hi, lo) boxes; later L1 (hi 0-3, lo 4-7) and the staged
 // update (8-11).
+static_assert(12 * kTileBytes + 8 * 8 + 2 * 4 + 1023 <= kSmemBytes,
+              "chain_tile_kernel: twelve tiles, eight barriers and two words after alignment");
+
 __global__ void __launch_bounds__(128, 1)
 chain_tile_kernel(const __grid_constant__ CUtensorMap l_hi, const __grid_constant__ CUtensorMap l_lo,
                   const __grid_constant__ CUtensorMap z_hi, const __grid_constant__ CUtensorMap z_lo,
