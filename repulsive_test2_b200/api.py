@@ -531,6 +531,32 @@ def sobolevStep(vertices, edges, disjointPairs, x0, opts=None):
     return sobolevStepSet(vertices, edges, disjointPairs, [barycenterBlock(x0)], opts)
 
 
+def step(vertices, edges, disjointPairs, opts):
+    """optimizer.ts:37-71: one raw L2 gradient-descent step.
+
+    grad (the device's analytic gradient when ``opts["mode"] == "analytical"``,
+    else its forward-difference gradient with step ``h``), then
+    ``vertices - stepSize * grad`` and the device energy of the result. Returns
+    ``{"vertices", "energy"}`` plus ``"field"`` (the gradient at the input
+    vertices) when ``collectField`` is set. Inputs are not modified.
+    """
+    def opt(key):
+        val = opts.get(key)
+        return DEFAULTS[key] if val is None else val
+
+    alpha, beta, epsilon, h = opt("alpha"), opt("beta"), opt("epsilon"), opt("h")
+    v = _v(vertices)
+    if opts.get("mode") == "analytical":
+        grad = gradientAnalytical(v, edges, disjointPairs, alpha, beta, epsilon)
+    else:
+        grad = gradientFiniteDiff(v, edges, disjointPairs, alpha, beta, epsilon, h)
+    nxt = v - float(opts["stepSize"]) * grad
+    out = {"vertices": nxt, "energy": calculateEnergy(nxt, edges, disjointPairs, alpha, beta, epsilon)}
+    if opts.get("collectField"):
+        out["field"] = grad
+    return out
+
+
 # ---- penalties.ts ---------------------------------------------------------------------
 
 def _pen(config) -> abi.tpe_penalties:

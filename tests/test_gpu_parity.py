@@ -271,3 +271,17 @@ def test_backstops_never_raise():
     r = T.sobolevStepSet(v, e, None, blocks)
     rc, out, st, _ = O.sobolev_step(v, e, blocks)
     assert r["accepted"] == bool(st.accepted) and r["stats"].get("reason") == abi.REASONS[st.reason]
+
+
+@pytest.mark.parametrize("mode", ["analytical", "finiteDiff"])
+def test_raw_gradient_step(mode):
+    """optimizer.ts:37-71 on the device: grad, v - stepSize*grad, energy(next)."""
+    v, e = F.trefoil(64, jitter=0.01, seed=64)
+    s = 1e-3
+    r = T.step(v, e, None, {"mode": mode, "stepSize": s, "collectField": True})
+    g = O.gradient(v, e) if mode == "analytical" else O.gradient_fd(v, e)
+    assert relerr(r["field"], g) <= (1e-10 if mode == "analytical" else 1e-6)
+    assert np.array_equal(r["vertices"], v - s * r["field"])
+    en = O.energy(r["vertices"], e)
+    assert abs(r["energy"] - en) <= 1e-10 * abs(en)
+    assert "field" not in T.step(v, e, None, {"mode": mode, "stepSize": s})
