@@ -1072,8 +1072,9 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
     const float* Zf = ctx->mx_Zd.as<float>();
     const float* Wf = ctx->mx_Wd.as<float>();
     std::vector<double> hres(kMaxRhs), hbn(kMaxRhs);
-    // squared residual norms per iteration, for the predicted stop below
-    std::vector<double> hist((size_t)(maxit > 0 ? maxit + 1 : 1) * kMaxRhs);
+    // squared residual norms of the last kRateSpan + 1 iterations (a ring), for
+    // the predicted stop below
+    std::vector<double> hist((size_t)(kRateSpan + 1) * kMaxRhs);
     int32_t max_iters = 0;
     const unsigned rb_V = (unsigned)((V + kMvRows - 1) / kMvRows);
     const unsigned rb_Vp = (unsigned)(Vp / kMvRows);
@@ -1143,13 +1144,15 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
             // From iteration kPredictFrom on, stop (not converged: the caller falls
             // back to the FP64 factorization) once a column's residual rate over
             // the last kRateSpan iterations predicts it reaches tol only after maxit.
-            std::copy(hres.begin(), hres.begin() + n, hist.begin() + (size_t)it * kMaxRhs);
+            std::copy(hres.begin(), hres.begin() + n,
+                      hist.begin() + (size_t)(it % (kRateSpan + 1)) * kMaxRhs);
             if (it >= kPredictFrom && it >= kRateSpan) {
                 bool hopeless = false;
                 for (int c = 0; c < n && !hopeless; c++) {
                     const double target = tol * tol * hbn[c];
                     if (hres[c] <= target) continue;
-                    const double now = hres[c], old = hist[(size_t)(it - kRateSpan) * kMaxRhs + c];
+                    const double now = hres[c],
+                                 old = hist[(size_t)((it - kRateSpan) % (kRateSpan + 1)) * kMaxRhs + c];
                     if (!(now < old) || !(now > 0.0)) {
                         hopeless = true;
                     } else {
