@@ -36,7 +36,8 @@ enum {
     TPE_ERR_INVALID_SET = 7,      /* totalLength + edgeLengths in one set (constraintSet.ts:333-344) */
     TPE_ERR_REFINE_NOT_CONVERGED = 8, /* mixed path: the FP64 CG hit its cap */
     TPE_ERR_DEVICE_TIMEOUT = 9,   /* a bounded device-side wait gave up */
-    TPE_ERR_TOO_LARGE = 10        /* request exceeds a fixed-capacity buffer */
+    TPE_ERR_TOO_LARGE = 10,       /* request exceeds a fixed-capacity buffer */
+    TPE_ERR_INTERNAL = 11         /* a host-side C++ exception; see tpe_last_error */
 };
 
 /* ---- step outcome reasons (optimizer.ts:186, lineSearch.ts:374-379) ------- */

@@ -24,6 +24,7 @@ TPE_ERR_INVALID_SET = 7
 TPE_ERR_REFINE_NOT_CONVERGED = 8
 TPE_ERR_DEVICE_TIMEOUT = 9
 TPE_ERR_TOO_LARGE = 10
+TPE_ERR_INTERNAL = 11
 
 REASONS = {
     0: None,

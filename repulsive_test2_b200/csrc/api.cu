@@ -1226,7 +1226,11 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
         if (status) *status = TPE_ERR_CUDA;
         return nullptr;
     }
-    tpe_ctx* ctx = new tpe_ctx();
+    tpe_ctx* ctx = new (std::nothrow) tpe_ctx();
+    if (!ctx) {
+        if (status) *status = TPE_ERR_OUT_OF_MEMORY;
+        return nullptr;
+    }
     ctx->device = device;
     // The main stream carries the factorization's critical path: give it the
     // highest priority so its one-CTA kernels are dispatched ahead of everything
@@ -1302,289 +1306,315 @@ void tpe_destroy(tpe_ctx* ctx) {
 const char* tpe_last_error(const tpe_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 int32_t tpe_set_topology(tpe_ctx* ctx, const int32_t* edges, int32_t E, int32_t V) {
-    if (!ctx) return TPE_ERR_BAD_ARG;
-    if (E < 0 || V < 0 || (E > 0 && !edges)) {
-        set_error(ctx, TPE_ERR_BAD_ARG, "tpe_set_topology: bad sizes");
-        return TPE_ERR_BAD_ARG;
-    }
-    for (int64_t i = 0; i < 2 * (int64_t)E; i++)
-        if (edges[i] < 0 || edges[i] >= V) {
-            set_error(ctx, TPE_ERR_BAD_ARG, "tpe_set_topology: edge index out of range");
+    return guarded(ctx, [&]() -> int32_t {
+        if (!ctx) return TPE_ERR_BAD_ARG;
+        if (E < 0 || V < 0 || (E > 0 && !edges)) {
+            set_error(ctx, TPE_ERR_BAD_ARG, "tpe_set_topology: bad sizes");
             return TPE_ERR_BAD_ARG;
         }
-    TPE_CUDA_TRY(cudaSetDevice(ctx->device));
-    ctx->V = V;
-    ctx->E = E;
-    ctx->h_edges.assign(edges, edges + 2 * (size_t)E);
-    ctx->h_inc_off.assign((size_t)V + 1, 0);
-    for (int32_t I = 0; I < E; I++) {
-        ctx->h_inc_off[edges[2 * I] + 1]++;
-        ctx->h_inc_off[edges[2 * I + 1] + 1]++;
-    }
-    for (int32_t v = 0; v < V; v++) ctx->h_inc_off[v + 1] += ctx->h_inc_off[v];
-    ctx->h_inc.assign(2 * (size_t)E, 0);
-    std::vector<int32_t> fill(ctx->h_inc_off.begin(), ctx->h_inc_off.end() - 1);
-    for (int32_t I = 0; I < E; I++)
-        for (int s = 0; s < 2; s++) ctx->h_inc[fill[edges[2 * I + s]]++] = 2 * I + s;
-    TPE_TRY(upload(ctx, ctx->d_edges, ctx->h_edges.data(), sizeof(int32_t) * 2 * (size_t)(E > 0 ? E : 1)));
-    TPE_TRY(upload(ctx, ctx->d_inc_off, ctx->h_inc_off.data(), sizeof(int32_t) * ((size_t)V + 1)));
-    TPE_TRY(upload(ctx, ctx->d_inc, ctx->h_inc.data(), sizeof(int32_t) * 2 * (size_t)(E > 0 ? E : 1)));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    ctx->has_topology = true;
-    ctx->op.valid = false;
-    return TPE_OK;
+        for (int64_t i = 0; i < 2 * (int64_t)E; i++)
+            if (edges[i] < 0 || edges[i] >= V) {
+                set_error(ctx, TPE_ERR_BAD_ARG, "tpe_set_topology: edge index out of range");
+                return TPE_ERR_BAD_ARG;
+            }
+        TPE_CUDA_TRY(cudaSetDevice(ctx->device));
+        ctx->V = V;
+        ctx->E = E;
+        ctx->h_edges.assign(edges, edges + 2 * (size_t)E);
+        ctx->h_inc_off.assign((size_t)V + 1, 0);
+        for (int32_t I = 0; I < E; I++) {
+            ctx->h_inc_off[edges[2 * I] + 1]++;
+            ctx->h_inc_off[edges[2 * I + 1] + 1]++;
+        }
+        for (int32_t v = 0; v < V; v++) ctx->h_inc_off[v + 1] += ctx->h_inc_off[v];
+        ctx->h_inc.assign(2 * (size_t)E, 0);
+        std::vector<int32_t> fill(ctx->h_inc_off.begin(), ctx->h_inc_off.end() - 1);
+        for (int32_t I = 0; I < E; I++)
+            for (int s = 0; s < 2; s++) ctx->h_inc[fill[edges[2 * I + s]]++] = 2 * I + s;
+        TPE_TRY(upload(ctx, ctx->d_edges, ctx->h_edges.data(), sizeof(int32_t) * 2 * (size_t)(E > 0 ? E : 1)));
+        TPE_TRY(upload(ctx, ctx->d_inc_off, ctx->h_inc_off.data(), sizeof(int32_t) * ((size_t)V + 1)));
+        TPE_TRY(upload(ctx, ctx->d_inc, ctx->h_inc.data(), sizeof(int32_t) * 2 * (size_t)(E > 0 ? E : 1)));
+        TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        ctx->has_topology = true;
+        ctx->op.valid = false;
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_disjoint_pairs(tpe_ctx* ctx, int32_t* offsets, int32_t* partners, int64_t cap) {
-    TPE_TRY(check_topology(ctx));
-    const int32_t E = ctx->E;
-    const int32_t* ed = ctx->h_edges.data();
-    int64_t count = 0;
-    for (int32_t i = 0; i < E; i++) {
-        if (offsets) offsets[i] = (int32_t)count;
-        for (int32_t j = 0; j < E; j++) {
-            if (i == j) continue;
-            const int32_t a1 = ed[2 * i], a2 = ed[2 * i + 1], b1 = ed[2 * j], b2 = ed[2 * j + 1];
-            if (a1 != b1 && a1 != b2 && a2 != b1 && a2 != b2) {
-                if (partners && count < cap) partners[count] = j;
-                count++;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        const int32_t E = ctx->E;
+        const int32_t* ed = ctx->h_edges.data();
+        int64_t count = 0;
+        for (int32_t i = 0; i < E; i++) {
+            if (offsets) offsets[i] = (int32_t)count;
+            for (int32_t j = 0; j < E; j++) {
+                if (i == j) continue;
+                const int32_t a1 = ed[2 * i], a2 = ed[2 * i + 1], b1 = ed[2 * j], b2 = ed[2 * j + 1];
+                if (a1 != b1 && a1 != b2 && a2 != b1 && a2 != b2) {
+                    if (partners && count < cap) partners[count] = j;
+                    count++;
+                }
             }
         }
-    }
-    if (offsets) offsets[E] = (int32_t)count;
-    if (partners && count > cap) {
-        set_error(ctx, TPE_ERR_TOO_LARGE, "tpe_disjoint_pairs: partners capacity too small");
-        return TPE_ERR_TOO_LARGE;
-    }
-    return TPE_OK;
+        if (offsets) offsets[E] = (int32_t)count;
+        if (partners && count > cap) {
+            set_error(ctx, TPE_ERR_TOO_LARGE, "tpe_disjoint_pairs: partners capacity too small");
+            return TPE_ERR_TOO_LARGE;
+        }
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_energy(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double* energy) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !p || !energy) return TPE_ERR_BAD_ARG;
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)ctx->V));
-    return energy_of(ctx, ctx->pos.as<double>(), p->alpha, p->beta, p->epsilon, energy);
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !p || !energy) return TPE_ERR_BAD_ARG;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)ctx->V));
+        return energy_of(ctx, ctx->pos.as<double>(), p->alpha, p->beta, p->epsilon, energy);
+    });
 }
 
 int32_t tpe_energy_grad(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double* energy,
                         double* grad) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !p) return TPE_ERR_BAD_ARG;
-    const int32_t V = ctx->V;
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
-    TPE_TRY(ensure(ctx, ctx->grad, sizeof(double) * 3 * (size_t)(V > 0 ? V : 1)));
-    TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * 600));
-    TPE_TRY(edge_prep(ctx, ctx->pos.as<double>(), 1, p->epsilon, p->alpha));
-    double* de = ctx->scalars.as<double>() + 530;
-    TPE_TRY(energy_grad_fp64(ctx, p->alpha, p->beta, p->epsilon, energy ? de : nullptr,
-                             grad ? ctx->grad.as<double>() : nullptr));
-    if (grad) TPE_TRY(download(ctx, grad, ctx->grad.ptr, sizeof(double) * 3 * (size_t)V));
-    if (energy) TPE_TRY(download(ctx, energy, de, sizeof(double)));
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !p) return TPE_ERR_BAD_ARG;
+        const int32_t V = ctx->V;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
+        TPE_TRY(ensure(ctx, ctx->grad, sizeof(double) * 3 * (size_t)(V > 0 ? V : 1)));
+        TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * 600));
+        TPE_TRY(edge_prep(ctx, ctx->pos.as<double>(), 1, p->epsilon, p->alpha));
+        double* de = ctx->scalars.as<double>() + 530;
+        TPE_TRY(energy_grad_fp64(ctx, p->alpha, p->beta, p->epsilon, energy ? de : nullptr,
+                                 grad ? ctx->grad.as<double>() : nullptr));
+        if (grad) TPE_TRY(download(ctx, grad, ctx->grad.ptr, sizeof(double) * 3 * (size_t)V));
+        if (energy) TPE_TRY(download(ctx, energy, de, sizeof(double)));
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_gradient_fd(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double h,
                         double* grad) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !p || !grad) return TPE_ERR_BAD_ARG;
-    const int32_t V = ctx->V;
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
-    TPE_TRY(ensure(ctx, ctx->grad, sizeof(double) * 3 * (size_t)V));
-    TPE_TRY(gradient_fd_dev(ctx, ctx->pos.as<double>(), p->alpha, p->beta, p->epsilon, h,
-                            ctx->grad.as<double>()));
-    return download(ctx, grad, ctx->grad.ptr, sizeof(double) * 3 * (size_t)V);
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !p || !grad) return TPE_ERR_BAD_ARG;
+        const int32_t V = ctx->V;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
+        TPE_TRY(ensure(ctx, ctx->grad, sizeof(double) * 3 * (size_t)V));
+        TPE_TRY(gradient_fd_dev(ctx, ctx->pos.as<double>(), p->alpha, p->beta, p->epsilon, h,
+                                ctx->grad.as<double>()));
+        return download(ctx, grad, ctx->grad.ptr, sizeof(double) * 3 * (size_t)V);
+    });
 }
 
 int32_t tpe_assemble(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double* B_out,
                      double* B0_out, double* A_out) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !p) return TPE_ERR_BAD_ARG;
-    const int32_t V = ctx->V;
-    const size_t nn = (size_t)V * V;
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
-    TPE_TRY(ensure(ctx, ctx->mat_A, sizeof(double) * nn));
-    if (B_out) TPE_TRY(ensure(ctx, ctx->mat_B, sizeof(double) * nn));
-    if (B0_out) TPE_TRY(ensure(ctx, ctx->mat_B0, sizeof(double) * nn));
-    TPE_TRY(edge_prep(ctx, ctx->pos.as<double>(), 1, p->epsilon, p->alpha));
-    TPE_TRY(assemble_fp64(ctx, p->alpha, p->beta, p->epsilon, ctx->mat_A.as<double>(),
-                          B_out ? ctx->mat_B.as<double>() : nullptr,
-                          B0_out ? ctx->mat_B0.as<double>() : nullptr));
-    ctx->op.valid = false;
-    if (A_out) TPE_TRY(download(ctx, A_out, ctx->mat_A.ptr, sizeof(double) * nn));
-    if (B_out) TPE_TRY(download(ctx, B_out, ctx->mat_B.ptr, sizeof(double) * nn));
-    if (B0_out) TPE_TRY(download(ctx, B0_out, ctx->mat_B0.ptr, sizeof(double) * nn));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !p) return TPE_ERR_BAD_ARG;
+        const int32_t V = ctx->V;
+        const size_t nn = (size_t)V * V;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
+        TPE_TRY(ensure(ctx, ctx->mat_A, sizeof(double) * nn));
+        if (B_out) TPE_TRY(ensure(ctx, ctx->mat_B, sizeof(double) * nn));
+        if (B0_out) TPE_TRY(ensure(ctx, ctx->mat_B0, sizeof(double) * nn));
+        TPE_TRY(edge_prep(ctx, ctx->pos.as<double>(), 1, p->epsilon, p->alpha));
+        TPE_TRY(assemble_fp64(ctx, p->alpha, p->beta, p->epsilon, ctx->mat_A.as<double>(),
+                              B_out ? ctx->mat_B.as<double>() : nullptr,
+                              B0_out ? ctx->mat_B0.as<double>() : nullptr));
+        ctx->op.valid = false;
+        if (A_out) TPE_TRY(download(ctx, A_out, ctx->mat_A.ptr, sizeof(double) * nn));
+        if (B_out) TPE_TRY(download(ctx, B_out, ctx->mat_B.ptr, sizeof(double) * nn));
+        if (B0_out) TPE_TRY(download(ctx, B0_out, ctx->mat_B0.ptr, sizeof(double) * nn));
+        TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_constraint_rows(const tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks) {
-    if (!ctx || (nblocks > 0 && !set)) return -1;
-    int32_t k = 0;
-    for (int32_t b = 0; b < nblocks; b++) {
-        switch (set[b].kind) {
-            case TPE_BLOCK_BARYCENTER:
-            case TPE_BLOCK_POINT: k += 3; break;
-            case TPE_BLOCK_TOTAL_LENGTH: k += 1; break;
-            case TPE_BLOCK_EDGE_LENGTHS: k += ctx->E; break;
-            default: return -1;
+    return guarded(nullptr, [&]() -> int32_t {
+        if (!ctx || (nblocks > 0 && !set)) return -1;
+        int32_t k = 0;
+        for (int32_t b = 0; b < nblocks; b++) {
+            switch (set[b].kind) {
+                case TPE_BLOCK_BARYCENTER:
+                case TPE_BLOCK_POINT: k += 3; break;
+                case TPE_BLOCK_TOTAL_LENGTH: k += 1; break;
+                case TPE_BLOCK_EDGE_LENGTHS: k += ctx->E; break;
+                default: return -1;
+            }
         }
-    }
-    return k;
+        return k;
+    });
 }
 
 int32_t tpe_evaluate_constraints(tpe_ctx* ctx, const double* xyz, const tpe_constraint* set,
                                  int32_t nblocks, double* phi, double* C) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !phi) return TPE_ERR_BAD_ARG;
-    const int32_t V = ctx->V;
-    SetInfo S;
-    TPE_TRY(set_k(ctx, set, nblocks, &S));
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
-    if (C) TPE_TRY(ensure(ctx, ctx->con_C, sizeof(double) * (size_t)(S.k > 0 ? S.k : 1) * 3 * V));
-    std::vector<double> ph, ns;
-    TPE_TRY(eval_constraints(ctx, ctx->pos.as<double>(), nblocks, S.k,
-                             C ? ctx->con_C.as<double>() : nullptr, ph, ns));
-    ctx->op.valid = false;
-    if (S.k > 0) memcpy(phi, ph.data(), sizeof(double) * S.k);
-    if (C && S.k > 0)
-        TPE_TRY(download(ctx, C, ctx->con_C.ptr, sizeof(double) * (size_t)S.k * 3 * V));
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !phi) return TPE_ERR_BAD_ARG;
+        const int32_t V = ctx->V;
+        SetInfo S;
+        TPE_TRY(set_k(ctx, set, nblocks, &S));
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
+        if (C) TPE_TRY(ensure(ctx, ctx->con_C, sizeof(double) * (size_t)(S.k > 0 ? S.k : 1) * 3 * V));
+        std::vector<double> ph, ns;
+        TPE_TRY(eval_constraints(ctx, ctx->pos.as<double>(), nblocks, S.k,
+                                 C ? ctx->con_C.as<double>() : nullptr, ph, ns));
+        ctx->op.valid = false;
+        if (S.k > 0) memcpy(phi, ph.data(), sizeof(double) * S.k);
+        if (C && S.k > 0)
+            TPE_TRY(download(ctx, C, ctx->con_C.ptr, sizeof(double) * (size_t)S.k * 3 * V));
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_l2_curve_norm(tpe_ctx* ctx, const double* values, const double* xyz, double* out) {
-    TPE_TRY(check_topology(ctx));
-    if (!values || !xyz || !out) return TPE_ERR_BAD_ARG;
-    const int32_t V = ctx->V;
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
-    TPE_TRY(upload(ctx, ctx->grad, values, sizeof(double) * 3 * (size_t)V));
-    return l2_curve_norm(ctx, ctx->grad.as<double>(), ctx->pos.as<double>(), out);
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!values || !xyz || !out) return TPE_ERR_BAD_ARG;
+        const int32_t V = ctx->V;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)V));
+        TPE_TRY(upload(ctx, ctx->grad, values, sizeof(double) * 3 * (size_t)V));
+        return l2_curve_norm(ctx, ctx->grad.as<double>(), ctx->pos.as<double>(), out);
+    });
 }
 
 int32_t tpe_solve_saddle(tpe_ctx* ctx, const double* A, int32_t n, const double* C, int32_t k,
                          const double* rhs_top, const double* rhs_bottom, int32_t factor_mode,
                          double* x, double* lambda, double* residual) {
-    (void)factor_mode;  // the structured Cholesky solve serves both factor modes
-    if (!ctx || !A || n <= 0 || k < 0 || (k > 0 && !C) || !rhs_top || !x) return TPE_ERR_BAD_ARG;
-    TPE_CUDA_TRY(cudaSetDevice(ctx->device));
-    const size_t m = 3 * (size_t)n;
-    if (!all_finite(rhs_top, m) || (rhs_bottom && !all_finite(rhs_bottom, (size_t)k))) {
-        set_error(ctx, TPE_ERR_NONFINITE_INPUT, "non-finite right-hand side: treating as singular");
-        return TPE_ERR_NONFINITE_INPUT;
-    }
-    TPE_TRY(upload(ctx, ctx->mat_A, A, sizeof(double) * (size_t)n * n));
-    TPE_TRY(ensure(ctx, ctx->con_C, sizeof(double) * (size_t)(k > 0 ? k : 1) * m));
-    if (k > 0) TPE_TRY(upload(ctx, ctx->con_C, C, sizeof(double) * (size_t)k * m));
-    TPE_TRY(upload(ctx, ctx->flat2, rhs_top, sizeof(double) * m));
-    bool singular = false;
-    TPE_TRY(op_finalize(ctx, n, k, &singular, ctx->flat2.as<double>()));
-    if (singular) {
-        set_error(ctx, TPE_ERR_SINGULAR, "saddle system is singular");
-        return TPE_ERR_SINGULAR;
-    }
-    TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
-    std::vector<double> lam;
-    double res = 0.0;
-    TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), rhs_bottom, ctx->flat1.as<double>(), lam, &res));
-    TPE_TRY(download(ctx, x, ctx->flat1.ptr, sizeof(double) * m));
-    if (lambda && k > 0) memcpy(lambda, lam.data(), sizeof(double) * k);
-    if (residual) *residual = res;
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        (void)factor_mode;  // the structured Cholesky solve serves both factor modes
+        if (!ctx || !A || n <= 0 || k < 0 || (k > 0 && !C) || !rhs_top || !x) return TPE_ERR_BAD_ARG;
+        TPE_CUDA_TRY(cudaSetDevice(ctx->device));
+        const size_t m = 3 * (size_t)n;
+        if (!all_finite(rhs_top, m) || (rhs_bottom && !all_finite(rhs_bottom, (size_t)k))) {
+            set_error(ctx, TPE_ERR_NONFINITE_INPUT, "non-finite right-hand side: treating as singular");
+            return TPE_ERR_NONFINITE_INPUT;
+        }
+        TPE_TRY(upload(ctx, ctx->mat_A, A, sizeof(double) * (size_t)n * n));
+        TPE_TRY(ensure(ctx, ctx->con_C, sizeof(double) * (size_t)(k > 0 ? k : 1) * m));
+        if (k > 0) TPE_TRY(upload(ctx, ctx->con_C, C, sizeof(double) * (size_t)k * m));
+        TPE_TRY(upload(ctx, ctx->flat2, rhs_top, sizeof(double) * m));
+        bool singular = false;
+        TPE_TRY(op_finalize(ctx, n, k, &singular, ctx->flat2.as<double>()));
+        if (singular) {
+            set_error(ctx, TPE_ERR_SINGULAR, "saddle system is singular");
+            return TPE_ERR_SINGULAR;
+        }
+        TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
+        std::vector<double> lam;
+        double res = 0.0;
+        TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), rhs_bottom, ctx->flat1.as<double>(), lam, &res));
+        TPE_TRY(download(ctx, x, ctx->flat1.ptr, sizeof(double) * m));
+        if (lambda && k > 0) memcpy(lambda, lam.data(), sizeof(double) * k);
+        if (residual) *residual = res;
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_solve_constrained_gradient(tpe_ctx* ctx, const double* xyz, const double* dE,
                                        const tpe_constraint* set, int32_t nblocks,
                                        const tpe_step_opts* o, double* g_tilde, double* lambda,
                                        double* residual) {
-    TPE_TRY(check_topology(ctx));
-    TPE_TRY(validate_opts(ctx, o));
-    if (!xyz || !dE || !g_tilde) return TPE_ERR_BAD_ARG;
-    const int32_t V = ctx->V;
-    const size_t m = 3 * (size_t)V;
-    SetInfo S;
-    TPE_TRY(set_k(ctx, set, nblocks, &S));
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
-    TPE_TRY(upload(ctx, ctx->grad, dE, sizeof(double) * m));
-    TPE_TRY(ensure(ctx, ctx->flat2, sizeof(double) * m));
-    TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
-    TPE_TRY(interleaved_to_block(ctx, ctx->grad.as<double>(), ctx->flat2.as<double>(), V));
-    bool singular = false;
-    TPE_TRY(op_build(ctx, ctx->pos.as<double>(), nblocks, S.k, o->alpha, o->beta, o->epsilon,
-                     &singular, nullptr, ctx->flat2.as<double>()));
-    if (singular) {
-        set_error(ctx, TPE_ERR_SINGULAR, "saddle system is singular");
-        return TPE_ERR_SINGULAR;
-    }
-    std::vector<double> lam;
-    double res = 0.0;
-    TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), nullptr, ctx->flat1.as<double>(), lam, &res));
-    TPE_TRY(block_to_interleaved(ctx, ctx->flat1.as<double>(), ctx->grad.as<double>(), V));
-    TPE_TRY(download(ctx, g_tilde, ctx->grad.ptr, sizeof(double) * m));
-    if (lambda && S.k > 0) memcpy(lambda, lam.data(), sizeof(double) * S.k);
-    if (residual) *residual = res;
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        TPE_TRY(validate_opts(ctx, o));
+        if (!xyz || !dE || !g_tilde) return TPE_ERR_BAD_ARG;
+        const int32_t V = ctx->V;
+        const size_t m = 3 * (size_t)V;
+        SetInfo S;
+        TPE_TRY(set_k(ctx, set, nblocks, &S));
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
+        TPE_TRY(upload(ctx, ctx->grad, dE, sizeof(double) * m));
+        TPE_TRY(ensure(ctx, ctx->flat2, sizeof(double) * m));
+        TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
+        TPE_TRY(interleaved_to_block(ctx, ctx->grad.as<double>(), ctx->flat2.as<double>(), V));
+        bool singular = false;
+        TPE_TRY(op_build(ctx, ctx->pos.as<double>(), nblocks, S.k, o->alpha, o->beta, o->epsilon,
+                         &singular, nullptr, ctx->flat2.as<double>()));
+        if (singular) {
+            set_error(ctx, TPE_ERR_SINGULAR, "saddle system is singular");
+            return TPE_ERR_SINGULAR;
+        }
+        std::vector<double> lam;
+        double res = 0.0;
+        TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), nullptr, ctx->flat1.as<double>(), lam, &res));
+        TPE_TRY(block_to_interleaved(ctx, ctx->flat1.as<double>(), ctx->grad.as<double>(), V));
+        TPE_TRY(download(ctx, g_tilde, ctx->grad.ptr, sizeof(double) * m));
+        if (lambda && S.k > 0) memcpy(lambda, lam.data(), sizeof(double) * S.k);
+        if (residual) *residual = res;
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_project(tpe_ctx* ctx, const double* xyz, const tpe_constraint* set, int32_t nblocks,
                     const tpe_step_opts* o, const double* base_xyz, double* xyz_out, int32_t* ok,
                     int32_t* iterations, double* phi_norm) {
-    TPE_TRY(check_topology(ctx));
-    TPE_TRY(validate_opts(ctx, o));
-    if (!xyz || !xyz_out || !ok || !iterations || !phi_norm) return TPE_ERR_BAD_ARG;
-    const int32_t V = ctx->V;
-    const size_t m = 3 * (size_t)V;
-    SetInfo S;
-    TPE_TRY(set_k(ctx, set, nblocks, &S));
-    if (base_xyz) {
-        TPE_TRY(upload(ctx, ctx->pos, base_xyz, sizeof(double) * m));
-        bool singular = false;
-        TPE_TRY(op_build(ctx, ctx->pos.as<double>(), nblocks, S.k, o->alpha, o->beta, o->epsilon,
-                         &singular, nullptr));
-        if (singular) {
-            set_error(ctx, TPE_ERR_SINGULAR, "frozen operator is singular");
-            return TPE_ERR_SINGULAR;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        TPE_TRY(validate_opts(ctx, o));
+        if (!xyz || !xyz_out || !ok || !iterations || !phi_norm) return TPE_ERR_BAD_ARG;
+        const int32_t V = ctx->V;
+        const size_t m = 3 * (size_t)V;
+        SetInfo S;
+        TPE_TRY(set_k(ctx, set, nblocks, &S));
+        if (base_xyz) {
+            TPE_TRY(upload(ctx, ctx->pos, base_xyz, sizeof(double) * m));
+            bool singular = false;
+            TPE_TRY(op_build(ctx, ctx->pos.as<double>(), nblocks, S.k, o->alpha, o->beta, o->epsilon,
+                             &singular, nullptr));
+            if (singular) {
+                set_error(ctx, TPE_ERR_SINGULAR, "frozen operator is singular");
+                return TPE_ERR_SINGULAR;
+            }
         }
-    }
-    TPE_TRY(upload(ctx, ctx->pos3, xyz, sizeof(double) * m));
-    TPE_TRY(ensure(ctx, ctx->pos2, sizeof(double) * m));
-    TPE_TRY(project_dev(ctx, ctx->pos3.as<double>(), S, o, base_xyz != nullptr,
-                        ctx->pos2.as<double>(), ok, iterations, phi_norm, nullptr));
-    return download(ctx, xyz_out, ctx->pos2.ptr, sizeof(double) * m);
+        TPE_TRY(upload(ctx, ctx->pos3, xyz, sizeof(double) * m));
+        TPE_TRY(ensure(ctx, ctx->pos2, sizeof(double) * m));
+        TPE_TRY(project_dev(ctx, ctx->pos3.as<double>(), S, o, base_xyz != nullptr,
+                            ctx->pos2.as<double>(), ok, iterations, phi_norm, nullptr));
+        return download(ctx, xyz_out, ctx->pos2.ptr, sizeof(double) * m);
+    });
 }
 
 int32_t tpe_line_search_step(tpe_ctx* ctx, const double* xyz, const double* dE,
                              const double* g_tilde, const tpe_constraint* set, int32_t nblocks,
                              const tpe_step_opts* o, double* xyz_out, tpe_step_stats* st) {
-    TPE_TRY(check_topology(ctx));
-    TPE_TRY(validate_opts(ctx, o));
-    if (!xyz || !dE || !g_tilde || !xyz_out || !st) return TPE_ERR_BAD_ARG;
-    stats_reset(st);
-    const int32_t V = ctx->V;
-    const size_t m = 3 * (size_t)V;
-    SetInfo S;
-    TPE_TRY(set_k(ctx, set, nblocks, &S));
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
-    TPE_TRY(upload(ctx, ctx->grad, dE, sizeof(double) * m));
-    TPE_TRY(upload(ctx, ctx->flat3, g_tilde, sizeof(double) * m));
-    const bool frozen = o->projection_mode == TPE_PROJECTION_FROZEN;
-    if (frozen) {
-        bool singular = false;
-        TPE_TRY(op_build(ctx, ctx->pos.as<double>(), nblocks, S.k, o->alpha, o->beta, o->epsilon,
-                         &singular, nullptr));
-        if (singular) {
-            set_error(ctx, TPE_ERR_SINGULAR, "frozen operator is singular");
-            return TPE_ERR_SINGULAR;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        TPE_TRY(validate_opts(ctx, o));
+        if (!xyz || !dE || !g_tilde || !xyz_out || !st) return TPE_ERR_BAD_ARG;
+        stats_reset(st);
+        const int32_t V = ctx->V;
+        const size_t m = 3 * (size_t)V;
+        SetInfo S;
+        TPE_TRY(set_k(ctx, set, nblocks, &S));
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
+        TPE_TRY(upload(ctx, ctx->grad, dE, sizeof(double) * m));
+        TPE_TRY(upload(ctx, ctx->flat3, g_tilde, sizeof(double) * m));
+        const bool frozen = o->projection_mode == TPE_PROJECTION_FROZEN;
+        if (frozen) {
+            bool singular = false;
+            TPE_TRY(op_build(ctx, ctx->pos.as<double>(), nblocks, S.k, o->alpha, o->beta, o->epsilon,
+                             &singular, nullptr));
+            if (singular) {
+                set_error(ctx, TPE_ERR_SINGULAR, "frozen operator is singular");
+                return TPE_ERR_SINGULAR;
+            }
         }
-    }
-    // flat3 is reused by the penalty kernels; keep g~ in a dedicated buffer
-    TPE_TRY(ensure(ctx, ctx->rhs, sizeof(double) * m));
-    TPE_CUDA_TRY(cudaMemcpyAsync(ctx->rhs.ptr, ctx->flat3.ptr, sizeof(double) * m,
-                                 cudaMemcpyDeviceToDevice, ctx->stream));
-    TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * (m + 16)));
-    TPE_TRY(ensure(ctx, ctx->sol, sizeof(double) * m));
-    double* out = ctx->sol.as<double>();
-    TPE_TRY(line_search_dev(ctx, ctx->pos.as<double>(), ctx->grad.as<double>(),
-                            ctx->rhs.as<double>(), S, o, frozen, out, st, nullptr));
-    return download(ctx, xyz_out, out, sizeof(double) * m);
+        // flat3 is reused by the penalty kernels; keep g~ in a dedicated buffer
+        TPE_TRY(ensure(ctx, ctx->rhs, sizeof(double) * m));
+        TPE_CUDA_TRY(cudaMemcpyAsync(ctx->rhs.ptr, ctx->flat3.ptr, sizeof(double) * m,
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+        TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double) * (m + 16)));
+        TPE_TRY(ensure(ctx, ctx->sol, sizeof(double) * m));
+        double* out = ctx->sol.as<double>();
+        TPE_TRY(line_search_dev(ctx, ctx->pos.as<double>(), ctx->grad.as<double>(),
+                                ctx->rhs.as<double>(), S, o, frozen, out, st, nullptr));
+        return download(ctx, xyz_out, out, sizeof(double) * m);
+    });
 }
 
 }  // extern "C"
@@ -1702,116 +1732,130 @@ extern "C" {
 int32_t tpe_sobolev_step(tpe_ctx* ctx, const double* xyz, const tpe_constraint* set,
                          int32_t nblocks, const tpe_step_opts* o, double* xyz_out,
                          tpe_step_stats* st, double* timings, double* descent_field) {
-    TPE_TRY(check_topology(ctx));
-    TPE_TRY(validate_opts(ctx, o));
-    if (!xyz || !xyz_out || !st) return TPE_ERR_BAD_ARG;
-    stats_reset(st);
-    if (timings) memset(timings, 0, sizeof(double) * 2 * TPE_PHASE_COUNT);
-    const size_t m = 3 * (size_t)ctx->V;
-    const double* res = nullptr;
-    {
-        Timer tstep(ctx, timings, TPE_PHASE_STEP);
-        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
-        TPE_TRY(step_impl(ctx, set, nblocks, o, st, timings, descent_field, &res));
-        TPE_TRY(download(ctx, xyz_out, res, sizeof(double) * m));
-    }
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        TPE_TRY(validate_opts(ctx, o));
+        if (!xyz || !xyz_out || !st) return TPE_ERR_BAD_ARG;
+        stats_reset(st);
+        if (timings) memset(timings, 0, sizeof(double) * 2 * TPE_PHASE_COUNT);
+        const size_t m = 3 * (size_t)ctx->V;
+        const double* res = nullptr;
+        {
+            Timer tstep(ctx, timings, TPE_PHASE_STEP);
+            TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
+            TPE_TRY(step_impl(ctx, set, nblocks, o, st, timings, descent_field, &res));
+            TPE_TRY(download(ctx, xyz_out, res, sizeof(double) * m));
+        }
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_sobolev_step_device(tpe_ctx* ctx, const double* d_xyz, const tpe_constraint* set,
                                 int32_t nblocks, const tpe_step_opts* o, double* d_xyz_out,
                                 tpe_step_stats* st, double* timings) {
-    TPE_TRY(check_topology(ctx));
-    TPE_TRY(validate_opts(ctx, o));
-    if (!d_xyz || !d_xyz_out || !st) return TPE_ERR_BAD_ARG;
-    stats_reset(st);
-    if (timings) memset(timings, 0, sizeof(double) * 2 * TPE_PHASE_COUNT);
-    const size_t m = 3 * (size_t)ctx->V;
-    const double* res = nullptr;
-    {
-        Timer tstep(ctx, timings, TPE_PHASE_STEP);
-        TPE_TRY(ensure(ctx, ctx->pos, sizeof(double) * m));
-        TPE_CUDA_TRY(cudaMemcpyAsync(ctx->pos.ptr, d_xyz, sizeof(double) * m,
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
-        TPE_TRY(step_impl(ctx, set, nblocks, o, st, timings, nullptr, &res));
-        TPE_CUDA_TRY(cudaMemcpyAsync(d_xyz_out, res, sizeof(double) * m, cudaMemcpyDeviceToDevice,
-                                     ctx->stream));
-        TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    }
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        TPE_TRY(validate_opts(ctx, o));
+        if (!d_xyz || !d_xyz_out || !st) return TPE_ERR_BAD_ARG;
+        stats_reset(st);
+        if (timings) memset(timings, 0, sizeof(double) * 2 * TPE_PHASE_COUNT);
+        const size_t m = 3 * (size_t)ctx->V;
+        const double* res = nullptr;
+        {
+            Timer tstep(ctx, timings, TPE_PHASE_STEP);
+            TPE_TRY(ensure(ctx, ctx->pos, sizeof(double) * m));
+            TPE_CUDA_TRY(cudaMemcpyAsync(ctx->pos.ptr, d_xyz, sizeof(double) * m,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+            TPE_TRY(step_impl(ctx, set, nblocks, o, st, timings, nullptr, &res));
+            TPE_CUDA_TRY(cudaMemcpyAsync(d_xyz_out, res, sizeof(double) * m, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+            TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        }
+        return TPE_OK;
+    });
 }
 
 void* tpe_stream(tpe_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int32_t tpe_profile(tpe_ctx* ctx, int32_t on) {
-    if (!ctx) return TPE_ERR_BAD_ARG;
-    TPE_CUDA_TRY(cudaSetDevice(ctx->device));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    for (auto& p : ctx->prof_pending) {
-        ctx->prof_pool.push_back(p.a);
-        ctx->prof_pool.push_back(p.b);
-    }
-    ctx->prof_pending.clear();
-    for (int g = 0; g < TPE_KGROUP_COUNT; g++) ctx->prof_ms[g] = 0.0;
-    for (int g = 0; g <= TPE_KGROUP_COUNT; g++) ctx->prof_launches[g] = 0;
-    ctx->profiling = on != 0;
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        if (!ctx) return TPE_ERR_BAD_ARG;
+        TPE_CUDA_TRY(cudaSetDevice(ctx->device));
+        TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        for (auto& p : ctx->prof_pending) {
+            ctx->prof_pool.push_back(p.a);
+            ctx->prof_pool.push_back(p.b);
+        }
+        ctx->prof_pending.clear();
+        for (int g = 0; g < TPE_KGROUP_COUNT; g++) ctx->prof_ms[g] = 0.0;
+        for (int g = 0; g <= TPE_KGROUP_COUNT; g++) ctx->prof_launches[g] = 0;
+        ctx->profiling = on != 0;
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_profile_read(tpe_ctx* ctx, double* ms, int64_t* launches) {
-    if (!ctx) return TPE_ERR_BAD_ARG;
-    TPE_CUDA_TRY(cudaSetDevice(ctx->device));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    for (auto& p : ctx->prof_pending) {
-        float t = 0.0f;
-        if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ctx->prof_ms[p.group] += t;
-        ctx->prof_pool.push_back(p.a);
-        ctx->prof_pool.push_back(p.b);
-    }
-    ctx->prof_pending.clear();
-    cudaGetLastError();
-    if (ms)
-        for (int g = 0; g < TPE_KGROUP_COUNT; g++) ms[g] = ctx->prof_ms[g];
-    if (launches)
-        for (int g = 0; g <= TPE_KGROUP_COUNT; g++) launches[g] = ctx->prof_launches[g];
-    return TPE_OK;
+    return guarded(ctx, [&]() -> int32_t {
+        if (!ctx) return TPE_ERR_BAD_ARG;
+        TPE_CUDA_TRY(cudaSetDevice(ctx->device));
+        TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        for (auto& p : ctx->prof_pending) {
+            float t = 0.0f;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ctx->prof_ms[p.group] += t;
+            ctx->prof_pool.push_back(p.a);
+            ctx->prof_pool.push_back(p.b);
+        }
+        ctx->prof_pending.clear();
+        cudaGetLastError();
+        if (ms)
+            for (int g = 0; g < TPE_KGROUP_COUNT; g++) ms[g] = ctx->prof_ms[g];
+        if (launches)
+            for (int g = 0; g <= TPE_KGROUP_COUNT; g++) launches[g] = ctx->prof_launches[g];
+        return TPE_OK;
+    });
 }
 
 int32_t tpe_penalty_energy(tpe_ctx* ctx, const double* xyz, const tpe_penalties* pen,
                            double* energy) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !pen || !energy) return TPE_ERR_BAD_ARG;
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)ctx->V));
-    return penalty_energy_dev(ctx, ctx->pos.as<double>(), pen, energy);
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !pen || !energy) return TPE_ERR_BAD_ARG;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)ctx->V));
+        return penalty_energy_dev(ctx, ctx->pos.as<double>(), pen, energy);
+    });
 }
 
 int32_t tpe_penalty_gradient(tpe_ctx* ctx, const double* xyz, const tpe_penalties* pen,
                              double* grad) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !pen || !grad) return TPE_ERR_BAD_ARG;
-    const size_t m = 3 * (size_t)ctx->V;
-    TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
-    TPE_TRY(ensure(ctx, ctx->grad, sizeof(double) * m));
-    TPE_TRY(penalty_gradient_dev(ctx, ctx->pos.as<double>(), pen, ctx->grad.as<double>(), 0));
-    return download(ctx, grad, ctx->grad.ptr, sizeof(double) * m);
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !pen || !grad) return TPE_ERR_BAD_ARG;
+        const size_t m = 3 * (size_t)ctx->V;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * m));
+        TPE_TRY(ensure(ctx, ctx->grad, sizeof(double) * m));
+        TPE_TRY(penalty_gradient_dev(ctx, ctx->pos.as<double>(), pen, ctx->grad.as<double>(), 0));
+        return download(ctx, grad, ctx->grad.ptr, sizeof(double) * m);
+    });
 }
 
 int32_t tpe_energy_batch(tpe_ctx* ctx, const double* xyz, int32_t ncurves, const tpe_params* p,
                          int32_t precision, double* energies) {
-    TPE_TRY(check_topology(ctx));
-    if (!xyz || !p || !energies || ncurves <= 0) return TPE_ERR_BAD_ARG;
-    const size_t m = 3 * (size_t)ctx->V;
-    TPE_TRY(upload(ctx, ctx->pos3, xyz, sizeof(double) * m * ncurves));
-    TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * (600 + (size_t)ncurves)));
-    double* de = ctx->scalars.as<double>() + 600;
-    if (precision == TPE_PRECISION_MIXED) {
-        TPE_TRY(edge_prep_mixed(ctx, ctx->pos3.as<double>(), ncurves, p->epsilon, p->alpha));
-        TPE_TRY(energy_mixed(ctx, ncurves, p->alpha, p->beta, p->epsilon, de));
-    } else {
-        TPE_TRY(edge_prep(ctx, ctx->pos3.as<double>(), ncurves, p->epsilon, p->alpha));
-        TPE_TRY(energy_fp64(ctx, ncurves, p->alpha, p->beta, p->epsilon, de));
-    }
-    return download(ctx, energies, de, sizeof(double) * ncurves);
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !p || !energies || ncurves <= 0) return TPE_ERR_BAD_ARG;
+        const size_t m = 3 * (size_t)ctx->V;
+        TPE_TRY(upload(ctx, ctx->pos3, xyz, sizeof(double) * m * ncurves));
+        TPE_TRY(ensure(ctx, ctx->scalars, sizeof(double) * (600 + (size_t)ncurves)));
+        double* de = ctx->scalars.as<double>() + 600;
+        if (precision == TPE_PRECISION_MIXED) {
+            TPE_TRY(edge_prep_mixed(ctx, ctx->pos3.as<double>(), ncurves, p->epsilon, p->alpha));
+            TPE_TRY(energy_mixed(ctx, ncurves, p->alpha, p->beta, p->epsilon, de));
+        } else {
+            TPE_TRY(edge_prep(ctx, ctx->pos3.as<double>(), ncurves, p->epsilon, p->alpha));
+            TPE_TRY(energy_fp64(ctx, ncurves, p->alpha, p->beta, p->epsilon, de));
+        }
+        return download(ctx, energies, de, sizeof(double) * ncurves);
+    });
 }
 
 }  // extern "C"

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -179,6 +181,32 @@ struct KernelScope {
 };
 
 void set_error(tpe_ctx* ctx, int32_t code, const std::string& msg);
+
+// Runs the body of a C entry point. A C++ exception (a failed host allocation,
+// a thread that could not start) becomes an error status, with the message in
+// the context when there is one, instead of leaving through the C ABI.
+template <class F>
+int32_t guarded(tpe_ctx* ctx, F&& body) noexcept {
+    int32_t code = TPE_ERR_INTERNAL;
+    const char* msg = "unexpected host-side exception";
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        code = TPE_ERR_OUT_OF_MEMORY;
+        msg = "host allocation failed";
+    } catch (const std::length_error&) {
+        code = TPE_ERR_TOO_LARGE;
+        msg = "host buffer size out of range";
+    } catch (const std::exception& e) {
+        msg = e.what();
+    } catch (...) {
+    }
+    try {
+        set_error(ctx, code, msg);
+    } catch (...) {
+    }
+    return code;
+}
 int32_t ensure(tpe_ctx* ctx, DevBuf& b, size_t bytes);
 
 // ---- pair kernels (pair_kernels.cu) ----------------------------------------
