@@ -296,8 +296,9 @@ def solveSaddleFromA(a, n: int, Cm, rhsTop, rhsBottom=None, factorMode: str = "l
 
 
 def _opts(o: Optional[Dict[str, Any]] = None, **kw) -> abi.tpe_step_opts:
-    ctx = context()
-    op = abi.default_opts(ctx.lib)
+    """SobolevStepOptions (optimizer.ts:95-184) plus this library's extensions
+    as the C struct, starting from the library's defaults (a host-only call)."""
+    op = abi.default_opts()
     d = dict(o or {})
     d.update(kw)
     if "mode" in d:
