@@ -42,3 +42,27 @@ def test_total_and_edge_lengths_are_mutually_exclusive():
     T.assertValidConstraintSet([T.edgeLengthsBlock(T.edgeLengths(v, e)), T.pointBlock(0, v[0])])
     with pytest.raises(ValueError, match="mutually exclusive"):
         T.assertValidConstraintSet([T.totalLengthBlock(1.0), T.edgeLengthsBlock(T.edgeLengths(v, e))])
+
+
+def _oracle_pairs(e):
+    import ctypes as C
+    from repulsive_test2_b200 import abi
+    e = np.ascontiguousarray(np.asarray(e, dtype=np.int32))
+    E = len(e)
+    n = O.lib().tpeo_disjoint_pairs(e.ctypes.data_as(abi.ip), E, None, None, 0)
+    off = np.zeros(E + 1, dtype=np.int32)
+    part = np.zeros(max(n, 1), dtype=np.int32)
+    O.lib().tpeo_disjoint_pairs(e.ctypes.data_as(abi.ip), E, off.ctypes.data_as(abi.ip),
+                                part.ctypes.data_as(abi.ip), n)
+    return [part[off[i]:off[i + 1]].tolist() for i in range(E)]
+
+
+def test_disjoint_pairs_listing_matches_the_oracle():
+    """tangentPointEnergy.ts:33-47: for each edge, the edges sharing no vertex, in index order."""
+    closed = F.trefoil(24, jitter=0.0, seed=7)[1]
+    y = np.array([[0, 1], [1, 2], [2, 3], [1, 4], [4, 5], [5, 0], [3, 3]], dtype=np.int32)
+    for e in (closed, y):
+        got = T.calculateDisjointPairs(e)
+        assert got == _oracle_pairs(e)
+    # a closed polygon: every edge is disjoint from all but itself and its two neighbours
+    assert all(len(p) == len(closed) - 3 for p in T.calculateDisjointPairs(closed))
