@@ -148,6 +148,27 @@ def extras(args):
     return out
 
 
+def bench_config(V):
+    """The workload both arms run (same dict in the reference arm's line)."""
+    return {"workload": f"random-walk closed knot V=E={V}, [barycenter,totalLength] frozen at the initial "
+                        "curve, frozen projection, analytical dE; a descent trajectory, each step starting "
+                        "at the previous output with its energy as energyBefore (the app's loop)",
+            "V": V,
+            "l2": "working set larger than L2 (A is 537 MB, the FP32 factor and its inverse 1.6 GB)"}
+
+
+def host_info():
+    model = ""
+    try:
+        for line in open("/proc/cpuinfo", encoding="utf-8"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cpu": model, "logical_cores": os.cpu_count()}
+
+
 def workload(V):
     from repulsive_test2_b200 import api as T
     from repulsive_test2_b200 import fixtures as F
@@ -457,26 +478,37 @@ def run_repulsive(args):
     torch.cuda.synchronize(dev)
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
 
-    # accuracy of the mixed step against the FP64 step from the initial curve
+    # Mixed against FP64 along the trajectory. (a) Fed the same iterate: at every
+    # iterate x_i of the FP64 trajectory both steps start from x_i with E(x_i) as
+    # energyBefore, so each step's error is its own. (b) Free-running: the two
+    # timed trajectories side by side (their iterates drift apart once an
+    # accepted step size differs).
     acc = {}
     if rank == 0:
-        res = {}
-        for name, o in (("mixed", step_opts(T, args.precision)), ("fp64", step_opts(T, "fp64"))):
-            res[name] = T.sobolevStepSet(v, e, None, blocks,
-                                         {"projectionMode": "frozen", "precision": name if name == "fp64" else args.precision,
-                                          "trials": o.trials, "collectField": True})
-        rm, rf = res["mixed"], res["fp64"]
-        gm, gf = rm["descentField"], rf["descentField"]
-        acc = {"energy_rel_err": abs(rm["energy"] - rf["energy"]) / abs(rf["energy"]),
-               "projected_gradient_rel_err": float(np.linalg.norm(gm - gf) / np.linalg.norm(gf)),
-               "vertices_rel_err": float(np.linalg.norm(rm["vertices"] - rf["vertices"]) /
-                                         np.linalg.norm(rf["vertices"])),
-               "tau_equal": rm["stats"]["tau"] == rf["stats"]["tau"],
-               "saddle_residual": rm["stats"]["residual"],
-               "cg_iterations": rm["stats"]["refineIterations"],
-               "note": "energy_rel_err: the accepted energy after one step from the initial curve, "
-                       "mixed vs FP64 (both evaluate it with the FP64 pair kernels; FP32 pair terms would "
-                       "give 1.5e-7 here); the mixed mode differs from FP64 only in the saddle solve"}
+        x, eb = v.copy(), E0
+        per = []
+        for i in range(args.steps):
+            base = {"projectionMode": "frozen", "energyBefore": eb, "collectField": True}
+            rf = T.sobolevStepSet(x, e, None, blocks, dict(base, precision="fp64", trials=1))
+            rm = T.sobolevStepSet(x, e, None, blocks, dict(base, precision=args.precision,
+                                                             trials=int(o_mix.trials)))
+            gm, gf = rm["descentField"], rf["descentField"]
+            per.append({"energy": abs(rm["energy"] - rf["energy"]) / abs(rf["energy"]),
+                        "g": float(np.linalg.norm(gm - gf) / np.linalg.norm(gf)),
+                        "x": float(np.linalg.norm(rm["vertices"] - rf["vertices"]) / np.linalg.norm(rf["vertices"])),
+                        "tau_equal": rm["stats"]["tau"] == rf["stats"]["tau"],
+                        "cg": rm["stats"]["refineIterations"], "residual": rm["stats"]["residual"]})
+            if rf["accepted"]:
+                x, eb = rf["vertices"], rf["energy"]
+        acc = {"steps": len(per),
+               "energy_rel_err_max": max(p_["energy"] for p_ in per),
+               "projected_gradient_rel_err_max": max(p_["g"] for p_ in per),
+               "vertices_rel_err_max": max(p_["x"] for p_ in per),
+               "tau_equal_steps": sum(p_["tau_equal"] for p_ in per),
+               "saddle_residual_max": max(p_["residual"] for p_ in per),
+               "cg_iterations": [p_["cg"] for p_ in per],
+               "method": "both solves from every iterate of the FP64 trajectory (same x_i, same "
+                         "energyBefore); errors of the mixed step against the FP64 step"}
 
     if rank != 0:
         if dist:
@@ -556,6 +588,15 @@ def run_repulsive(args):
                 "taus": [x["tau"] for x in log], "cg_iterations": [x["refine"] for x in log],
                 "energy_last": log[-1]["energy"] if log else None}
 
+    # free-running: the two timed trajectories (b)
+    split = next((i for i, (a, b) in enumerate(zip(log_mix, log_64)) if a["tau"] != b["tau"]), None)
+    traj_cmp = {"first_step_with_different_tau": split,
+                "energy_last_rel_diff": (abs(log_mix[-1]["energy"] - log_64[-1]["energy"]) / abs(log_64[-1]["energy"])
+                                         if log_mix and log_64 else None),
+                "method": "the two timed trajectories, each step from its own previous output"}
+
+    # Key order: the long blocks first, the metric's comparison last (the end of
+    # the line is what a truncated log shows).
     out = {
         "metric": METRIC,
         "value": value,
@@ -569,19 +610,10 @@ def run_repulsive(args):
         "vs_baseline": None,
         "dtype": "f64+tf32x3" if args.precision == "mixed" else "f64",
         "data": "synthetic: seeded random-walk knot (splitmix64/Box-Muller), no dataset",
-        "config": {"workload": f"random-walk closed knot V=E={V}, [barycenter,totalLength] frozen at the "
-                               "initial curve, frozen projection, analytical dE; a descent trajectory of "
-                               "`steps` steps from the initial curve, each step starting at the previous "
-                               "output with its energy as energyBefore (the app's loop)",
-                   "V": V, "precision": args.precision,
-                   "line_search": "8 step sizes projected per batch" if args.precision == "mixed" else "sequential",
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "working set larger than L2 (A is 537 MB, the FP32 factor and its inverse 1.6 GB)"},
-        "fp64": {"value": value64, "unit": "steps/s", "ms_per_step": ms64 / steps,
-                 "config": "plain FP64 GPU step: FP64 Cholesky, one step size at a time", "trajectory": traj(log_64)},
-        "speedup_vs_fp64": value / value64,
-        "accuracy_vs_fp64": acc,
-        "trajectory": traj(log_mix),
+        "config": bench_config(V),
+        "arm": {"precision": args.precision,
+                "line_search": "8 step sizes projected per batch" if args.precision == "mixed" else "sequential",
+                "parallelism": "replicas" if world > 1 else "single"},
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 8 * 3 * V,
                 "d2h_bytes_per_step": 8 * 3 * V},
@@ -593,28 +625,72 @@ def run_repulsive(args):
     if not args.no_cpu_baseline and world == 1:
         t_cpu, desc, parts = cpu_step_estimate(v, e, blocks, {}, args.cpu_budget)
         out["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "steps/s", "cores": 1, "kind": "port",
-                               "sample": desc, "phases_s": {k: round(x, 3) for k, x in parts.items()}}
+                               "estimate": True, "sample": desc, "host": host_info(),
+                               "phases_s": {k: round(x, 3) for k, x in parts.items()}}
+    out["trajectory"] = traj(log_mix)
+    out["fp64"] = {"value": value64, "unit": "steps/s", "ms_per_step": ms64 / steps,
+                   "config": "plain FP64 GPU step: FP64 Cholesky, one step size at a time",
+                   "trajectory": traj(log_64)}
+    out["trajectory_vs_fp64"] = traj_cmp
+    out["accuracy_vs_fp64"] = acc
+    out["speedup_vs_fp64"] = value / value64
     print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
+def oracle_full_step(V):
+    """Wall time of one whole oracle step (the reference's algorithm, 1 thread)
+    on the same workload at a size it finishes in about a minute."""
+    sys.path.insert(0, os.path.join(HERE, "tests"))
+    import oracle_lib as O
+    from repulsive_test2_b200 import abi
+
+    v, e, blocks = workload(V)
+    o = O.default_opts(projection_mode=abi.PROJECTION_FROZEN, has_energy_before=1,
+                       energy_before=O.energy(v, e))
+    t0 = time.perf_counter()
+    rc, _out, st, _f = O.sobolev_step(v, e, blocks, o)
+    dt = time.perf_counter() - t0
+    return dt, {"rc": rc, "tau": st.tau, "trials_evaluated": st.trials_evaluated,
+                "projection_iterations": st.projection_iterations}
+
+
 def run_reference(args):
+    """The reference's CPU path (its algorithm restated in C, single-threaded like
+    the TypeScript it restates) on this workload. A whole V=8192 oracle step
+    takes 17-23 minutes, so each of the K steps is a bounded sample of it:
+    per-phase row samples of the pair work and a Bunch-Kaufman LDL^T at a smaller
+    order, scaled by exact operation counts to one full step (an estimate, and
+    labelled so). The model is checked in the same run against one whole oracle
+    step timed at V=2048."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    t_start = time.perf_counter()
     v, e, blocks = workload(args.V)
     per_step = max(2.0, min(30.0, 150.0 / max(1, args.steps)))
-    # warm-up: one small sample (the CPU has no compile/caching stage to warm)
-    cpu_step_estimate(v, e, blocks, {}, 1.0)
+    for _ in range(args.warmup):
+        cpu_step_estimate(v, e, blocks, {}, 0.5)
     t_total = 0.0
     desc = ""
+    ests = []
     for _ in range(args.steps):
         t, desc, _parts = cpu_step_estimate(v, e, blocks, {}, per_step)
+        ests.append(t)
         t_total += t
     value = args.steps / t_total
+    # the model against one whole step at V=2048
+    check = {}
+    if args.V > 2048:
+        vs, es, bs = workload(2048)
+        model_s, _d, _p = cpu_step_estimate(vs, es, bs, {}, per_step)
+        full_s, info = oracle_full_step(2048)
+        check = {"V": 2048, "measured_full_step_s": full_s, "model_s": model_s,
+                 "model_over_measured": model_s / full_s, "oracle_step": info}
+    wall = time.perf_counter() - t_start
     out = {
         "impl": "reference",
         "metric": METRIC,
@@ -629,11 +705,16 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic: seeded random-walk knot (splitmix64/Box-Muller), no dataset",
-        "config": {"workload": f"random-walk closed knot V=E={args.V}, [barycenter,totalLength] frozen at the "
-                               "initial curve, frozen projection, analytical dE, one sobolevStepSet per step "
-                               "(energyBefore supplied)", "V": args.V},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port", "sample": desc},
+        "config": bench_config(args.V),
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port", "estimate": True,
+                         "sample": desc + f"; {args.steps} such samples, one per step",
+                         "host": host_info()},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "estimate": {"kind": "estimate",
+                     "note": "each step's time is a full V=8192 step extrapolated from bounded samples, "
+                             "so steps x ms_per_step exceeds the wall time of this run",
+                     "wall_s": wall, "per_step_estimates_s": [round(x, 1) for x in ests],
+                     "model_check": check},
     }
     print(json.dumps(out), flush=True)
 

@@ -146,9 +146,11 @@ typedef struct tpe_ctx tpe_ctx;
 /* ---- context -------------------------------------------------------------- */
 int32_t tpe_abi_version(void);
 void tpe_default_step_opts(tpe_step_opts* opts);
-/* Creates a context bound to CUDA device `device` (one per host thread; the
- * TypeScript side holds one per Web Worker). Returns NULL on failure with
- * *status set. */
+/* Creates a context bound to CUDA device `device` (the TypeScript side holds
+ * one per Web Worker). Every entry point that takes a context holds that
+ * context's mutex for the whole call, so calls on one context from several
+ * host threads run one after another; tpe_destroy must not overlap them.
+ * Returns NULL on failure with *status set. */
 tpe_ctx* tpe_create(int32_t device, int32_t* status);
 void tpe_destroy(tpe_ctx* ctx);
 /* Message for the last non-OK status returned on this context. */
@@ -259,19 +261,24 @@ int32_t tpe_energy_batch(tpe_ctx* ctx, const double* xyz, int32_t ncurves, const
                          int32_t precision, double* energies);
 
 /* ---- allocation-free energy (no counterpart in the reference) --------------- */
-/* calculateEnergy for callers that cannot call cudaMalloc: a loop being
- * captured into a CUDA graph, an application whose device memory comes only
- * from its own allocator, a real-time loop that must not hit the allocator.
- * d_xyz (V x 3 FP64) and d_edges (E x 2 int32) are device pointers on the
- * current device, d_energy receives one double there; `stream` is a
- * cudaStream_t (NULL = the legacy default stream). No context is created and
- * nothing is allocated: the scratch is a static device array of about 1 MiB
- * that every GPU loading the library holds until exit, so E is limited to
- * 16384 (larger E returns TPE_ERR_TOO_LARGE). The first call on a device looks
- * up the scratch's device address (cudaGetSymbolAddress), so make that first
- * call before any stream capture. All calls share the one scratch array: calls
- * that overlap on the GPU (different streams, or different host threads)
- * race; serialise them. */
+/* calculateEnergy for callers that cannot call cudaMalloc: an application whose
+ * device memory all comes from its own allocator or pool, or a real-time loop
+ * that must never enter the driver's allocator (cudaMalloc/cudaFree can
+ * synchronise the device). d_xyz (V x 3 FP64) and d_edges (E x 2 int32) are
+ * device pointers on the current device, d_energy receives one double there;
+ * `stream` is a cudaStream_t (NULL = the legacy default stream). No context is
+ * created and nothing is allocated: the scratch is a static device array of
+ * about 1 MiB that every GPU loading the library holds until exit, so E is
+ * limited to 16384 (larger E returns TPE_ERR_TOO_LARGE before any launch).
+ * Edge indices must lie in [0, V): they are checked on the device, and an
+ * index outside that range leaves the curve's energy NaN (no access outside
+ * d_xyz). The first call on a device looks up the scratch's device address
+ * (cudaGetSymbolAddress) and keeps it for the life of the process, so make that
+ * first call before any stream capture, and do not use this entry point across
+ * a cudaDeviceReset. All calls share the one scratch array: calls that overlap
+ * on the GPU (different streams, or different host threads) race; serialise
+ * them. A CUDA error left pending by the caller's earlier launches is reported
+ * as TPE_ERR_CUDA (and cleared) by this call. */
 int32_t tpe_energy_noalloc(const double* d_xyz, const int32_t* d_edges, int32_t V, int32_t E,
                            const tpe_params* p, double* d_energy, void* stream);
 

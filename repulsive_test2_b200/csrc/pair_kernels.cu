@@ -150,6 +150,48 @@ __global__ void reduce_partials(const double* __restrict__ partial, int32_t npar
     }
 }
 
+// edge_prep_kernel for edge indices that were never checked on the host (the
+// allocation-free entry point): an endpoint outside [0, V) skips the position
+// loads, leaves a NaN record and sets *bad.
+__global__ void edge_prep_checked_kernel(const double* __restrict__ p, const int2* __restrict__ edges,
+                                         int32_t E, int32_t V, double eps, double alpha,
+                                         double4* __restrict__ ea, double4* __restrict__ eb,
+                                         int32_t* __restrict__ bad) {
+    const int32_t I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= E) return;
+    const int2 e = edges[I];
+    if (e.x < 0 || e.x >= V || e.y < 0 || e.y >= V) {
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+        ea[I] = make_double4(nan, nan, nan, nan);
+        eb[I] = make_double4(nan, nan, nan, nan);
+        atomicOr(bad, 1);
+        return;
+    }
+    const double x1 = p[3 * e.x], y1 = p[3 * e.x + 1], z1 = p[3 * e.x + 2];
+    const double x2 = p[3 * e.y], y2 = p[3 * e.y + 1], z2 = p[3 * e.y + 2];
+    const double ex = x2 - x1, ey = y2 - y1, ez = z2 - z1;
+    const double ell = sqrt(ex * ex + ey * ey + ez * ez) + eps;
+    ea[I] = make_double4(x1, y1, z1, ell);
+    eb[I] = make_double4(x2, y2, z2, pow(ell, 1.0 - alpha));
+}
+
+// reduce_partials for one curve, NaN when *bad is set.
+__global__ void reduce_partials_checked(const double* __restrict__ partial, int32_t nparts,
+                                        double scale, const int32_t* __restrict__ bad,
+                                        double* __restrict__ out) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int32_t i = threadIdx.x; i < nparts; i += blockDim.x) s += partial[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        out[0] = *bad ? __longlong_as_double(0x7ff8000000000000LL) : scale * t;
+    }
+}
+
 // ---- symmetric (tile-pair) forms ---------------------------------------------
 //
 // Each unordered pair {I, J} of edges is evaluated once: the grid covers the
@@ -568,16 +610,6 @@ int32_t reduce_partials_launch(tpe_ctx* ctx, const double* partial, int32_t npar
     return TPE_OK;
 }
 
-int32_t gather_vertex_grad_launch(tpe_ctx* ctx, const double* edge_acc, int32_t nchunks,
-                                  double* grad) {
-    KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-    gather_vertex_grad<<<(ctx->V + 127) / 128, 128, 0, ctx->stream>>>(
-        edge_acc, nchunks, ctx->E, ctx->d_inc_off.as<int32_t>(), ctx->d_inc.as<int32_t>(), ctx->V,
-        grad);
-    TPE_CUDA_TRY(cudaGetLastError());
-    return TPE_OK;
-}
-
 int32_t edge_prep(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps,
                   double alpha) {
     const int32_t E = ctx->E;
@@ -617,12 +649,17 @@ int32_t energy_fp64(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, do
 }
 
 // Energy of one curve with caller-provided scratch (no context, no allocation):
-// edge records ea/eb (E each) and partial[max_parts]. Returns TPE_ERR_TOO_LARGE if
-// the partials do not fit. The J range is split into at most 16 chunks.
+// edge records ea/eb (E each), partial[max_parts] and one int flag *bad.
+// Returns TPE_ERR_TOO_LARGE if the partials do not fit. The J range is split
+// into at most 16 chunks. The caller's edge indices are checked on the device
+// (this path has no host copy of them): an index outside [0, V) skips its
+// loads, sets *bad, and the energy comes out NaN. Each launch is checked on its
+// own; an error pending from the caller's earlier work is reported (and
+// cleared) by the first check.
 int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2* d_edges,
                             int32_t V, int32_t E, double alpha, double beta, double eps,
                             double4* ea, double4* eb, double* partial, int32_t max_parts,
-                            double* d_energy) {
+                            int32_t* bad, double* d_energy) {
     const int32_t xb = (E + kThreads - 1) / kThreads;
     int32_t ny = (E + kTile - 1) / kTile;
     ny = ny < 16 ? ny : 16;
@@ -630,8 +667,10 @@ int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2
     const int32_t nyy = (E + jchunk - 1) / jchunk;
     const int32_t nparts = xb * nyy;
     if (nparts > max_parts) return TPE_ERR_TOO_LARGE;
-    edge_prep_kernel<<<(E + 255) / 256, 256, 0, stream>>>(d_pos, d_edges, E, V, 1, eps, alpha, ea,
-                                                          eb);
+    if (cudaMemsetAsync(bad, 0, sizeof(int32_t), stream) != cudaSuccess) return TPE_ERR_CUDA;
+    edge_prep_checked_kernel<<<(E + 255) / 256, 256, 0, stream>>>(d_pos, d_edges, E, V, eps, alpha,
+                                                                  ea, eb, bad);
+    if (cudaGetLastError() != cudaSuccess) return TPE_ERR_CUDA;
     dim3 grid(xb, nyy, 1);
     if (exp_mode(alpha, beta) == 1)
         energy_kernel<1><<<grid, kThreads, 0, stream>>>(ea, eb, d_edges, E, jchunk, alpha, beta,
@@ -639,7 +678,8 @@ int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2
     else
         energy_kernel<0><<<grid, kThreads, 0, stream>>>(ea, eb, d_edges, E, jchunk, alpha, beta,
                                                         eps, partial);
-    reduce_partials<<<1, 256, 0, stream>>>(partial, nparts, 0.125, d_energy);
+    if (cudaGetLastError() != cudaSuccess) return TPE_ERR_CUDA;
+    reduce_partials_checked<<<1, 256, 0, stream>>>(partial, nparts, 0.125, bad, d_energy);
     return cudaGetLastError() == cudaSuccess ? TPE_OK : TPE_ERR_CUDA;
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -101,6 +102,10 @@ struct DevBlock {
 }  // namespace tpe
 
 struct tpe_ctx {
+    // Held by every entry point for the whole call (tpe::guarded): calls on one
+    // context from several host threads run one after another. Recursive, so an
+    // entry point may call another on the same context.
+    std::recursive_mutex mu;
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;           // look-ahead stream of the factorization
@@ -182,14 +187,17 @@ struct KernelScope {
 
 void set_error(tpe_ctx* ctx, int32_t code, const std::string& msg);
 
-// Runs the body of a C entry point. A C++ exception (a failed host allocation,
-// a thread that could not start) becomes an error status, with the message in
-// the context when there is one, instead of leaving through the C ABI.
+// Runs the body of a C entry point under the context's mutex (when there is a
+// context). A C++ exception (a failed host allocation, a thread that could not
+// start, a mutex that could not be taken) becomes an error status, with the
+// message in the context when there is one, instead of leaving through the C ABI.
 template <class F>
 int32_t guarded(tpe_ctx* ctx, F&& body) noexcept {
     int32_t code = TPE_ERR_INTERNAL;
     const char* msg = "unexpected host-side exception";
     try {
+        std::unique_lock<std::recursive_mutex> lock;
+        if (ctx) lock = std::unique_lock<std::recursive_mutex>(ctx->mu);
         return body();
     } catch (const std::bad_alloc&) {
         code = TPE_ERR_OUT_OF_MEMORY;
@@ -217,24 +225,23 @@ int32_t edge_prep(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps
 // d_energy[ncurves] (device).
 int32_t energy_fp64(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, double eps,
                     double* d_energy);
-// Energy of one curve with caller-provided scratch and stream (no context).
+// Energy of one curve with caller-provided scratch and stream (no context);
+// edge indices are checked on the device (*bad set, energy NaN).
 int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2* d_edges,
                             int32_t V, int32_t E, double alpha, double beta, double eps,
                             double4* ea, double4* eb, double* partial, int32_t max_parts,
-                            double* d_energy);
+                            int32_t* bad, double* d_energy);
 // Energy (optional) and gradient (interleaved V x 3) of one curve. max_blocks > 0
 // bounds the SMs the pair kernel occupies (one block per SM).
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
                          double* d_grad, int32_t max_blocks = 0);
 
-// ---- mixed precision pair kernels (pair_mixed.cu) ----------------------------
+// ---- mixed precision energy (pair_mixed.cu) ----------------------------------
+// FP32 pair terms, FP64 sums: tpe_energy_batch with TPE_PRECISION_MIXED only.
 int32_t edge_prep_mixed(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps,
                         double alpha);
 int32_t energy_mixed(tpe_ctx* ctx, int32_t ncurves, double alpha, double beta, double eps,
                      double* d_energy);
-int32_t energy_grad_mixed(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
-                          double* d_grad);
-int32_t assemble_mixed(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_A);
 
 // ---- assembly (assembly.cu) -----------------------------------------------
 // A (and optionally B, B0) V x V row-major FP64 from prepared edge records.

@@ -1,10 +1,10 @@
 """Regenerates the committed golden fixtures under tests/golden/.
 
-Run in a container that has the reference checkout (default /root/reference,
-override with REFERENCE_ROOT); the GPU box never runs this script, it only
-reads the JSON files it wrote:
+Run where a checkout of the reference repository exists, naming its root in
+REFERENCE_ROOT (required; there is no default); the GPU tests never run this
+script, they only read the JSON files it wrote:
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 
 Outputs
   energy_bitexact.json   the reference's test/golden.json cases (energy and
@@ -27,7 +27,7 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT", "")
 sys.path.insert(0, REPO)
 
 from repulsive_test2_b200 import fixtures  # noqa: E402
@@ -81,6 +81,9 @@ def _compact(golden):
 
 
 def main() -> int:
+    if not REF or not os.path.isdir(REF):
+        print("set REFERENCE_ROOT to the root of a reference checkout", file=sys.stderr)
+        return 2
     _dump(_load(os.path.join(REF, "test", "golden.json")), "energy_bitexact.json")
     for gname, fname in REF_GOLDENS:
         fx = _load(os.path.join(REF, "oracle", "fixtures", f"{fname}.json"))

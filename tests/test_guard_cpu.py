@@ -52,3 +52,52 @@ def test_guard_turns_exceptions_into_status(tmp_path):
         pytest.fail(r.stderr[-2000:])
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.strip() == "0", out.stdout + out.stderr
+
+
+MUTEX_PROGRAM = r"""
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <thread>
+#include "tpe_internal.h"
+namespace tpe {
+void set_error(tpe_ctx* ctx, int32_t, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+}
+}  // namespace tpe
+int main() {
+    using namespace tpe;
+    tpe_ctx* ctx = new tpe_ctx();
+    std::atomic<int> inside{0}, overlaps{0}, calls{0};
+    auto worker = [&]() {
+        for (int i = 0; i < 200; i++) {
+            guarded(ctx, [&]() -> int32_t {
+                if (inside.fetch_add(1) != 0) overlaps++;
+                // an entry point may call another on the same context
+                guarded(ctx, [&]() -> int32_t { return 0; });
+                std::this_thread::sleep_for(std::chrono::microseconds(50));
+                inside.fetch_sub(1);
+                calls++;
+                return 0;
+            });
+        }
+    };
+    std::thread a(worker), b(worker);
+    a.join();
+    b.join();
+    printf("%d %d\n", overlaps.load(), calls.load());
+    return overlaps.load() != 0 || calls.load() != 400;
+}
+"""
+
+
+def test_context_calls_from_two_threads_do_not_overlap(tmp_path):
+    src = tmp_path / "mutex.cu"
+    src.write_text(MUTEX_PROGRAM)
+    exe = tmp_path / "mutex"
+    r = subprocess.run([B.nvcc(), *B.ARCH, "-std=c++17", "-I", CSRC, str(src), "-o", str(exe), "-lpthread"],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.fail(r.stderr[-2000:])
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip() == "0 400", out.stdout + out.stderr
