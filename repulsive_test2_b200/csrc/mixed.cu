@@ -4,12 +4,14 @@
 // The FP64 path factors A_rho = A + (rho/V) 1 1^T (dense.cu) and back-substitutes.
 // Here the same SPD matrix is
 //   1. Jacobi-scaled, S = D A_rho D with D = diag(A_rho)^(-1/2), and rounded
-//      to FP32 (padded to Vp = 128 * 2^k rows with an identity block);
+//      to FP32 (padded to Vp, the next multiple of 128, with an identity block);
 //   2. factored S ~ L L^T in FP32: 128 x 128 diagonal blocks in one CTA
 //      (potrf128_kernel, which also inverts them), the panel solve and the
 //      trailing update as 3xTF32 tcgen05 GEMMs (tc_gemm.cu);
 //   3. inverted, Z = L^{-1}, by the recursive block formula
-//      Z21 = -Z22 L21 Z11, level by level with all blocks of a level batched
+//      Z21 = -Z22 L21 Z11: the rows split into a first part of 128 * 2^k rows
+//      (the largest such part below Vp) and the rest, recursively; inside a
+//      part of 128 * 2^k rows level by level, all blocks of a level batched
 //      into one tcgen05 GEMM; W = Z^T is kept beside Z so every product is an
 //      A * B^T of row-major operands;
 //   4. used as the preconditioner M = Z^T Z = (L L^T)^{-1} of a block CG on
@@ -431,6 +433,26 @@ __global__ void transpose_block_kernel(const float* __restrict__ zhi, const floa
     }
 }
 
+// W[c0 + c][r0 + r] = Z[r0 + r][c0 + c] (r < 32 gridDim.y, c < 32 gridDim.x),
+// split: the W12 = Z21^T of an uneven split of the inverse.
+__global__ void transpose_rect_kernel(const float* __restrict__ zhi, const float* __restrict__ zlo,
+                                      float* __restrict__ whi, float* __restrict__ wlo,
+                                      int32_t ld, int32_t r0, int32_t c0) {
+    __shared__ float th[32][33], tl[32][33];
+    const int32_t rb = r0 + blockIdx.y * 32, cb = c0 + blockIdx.x * 32;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const size_t o = (size_t)(rb + yy) * ld + cb + threadIdx.x;
+        th[yy][threadIdx.x] = zhi[o];
+        tl[yy][threadIdx.x] = zlo[o];
+    }
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const size_t o = (size_t)(cb + yy) * ld + rb + threadIdx.x;
+        whi[o] = th[threadIdx.x][yy];
+        wlo[o] = tl[threadIdx.x][yy];
+    }
+}
+
 // ---- block CG kernels (vectors are [nr][Vp] FP64, pad entries stay 0) ------
 
 // U = D P, s[c] = sum_j U[c][j]   (one block per column)
@@ -591,9 +613,10 @@ __global__ void factor_to_f32_kernel(const float* __restrict__ zhi, const float*
     if (ti <= tj) wf[t] = whi[t] + wlo[t];
 }
 
-// Wf[c][base + r] = Zf[base + r][c] (r, c < m): the top level's W12 = Z21^T in FP32.
+// Wf[c][base + r] = Zf[base + r][c] (r < 32 gridDim.y, c < 32 gridDim.x): the top
+// level's W12 = Z21^T in FP32.
 __global__ void transpose_f32_kernel(const float* __restrict__ zf, float* __restrict__ wf,
-                                     int32_t ld, int32_t m, int32_t base) {
+                                     int32_t ld, int32_t base) {
     __shared__ float t[32][33];
     const int32_t r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
     for (int yy = threadIdx.y; yy < 32; yy += blockDim.y)
@@ -710,11 +733,18 @@ int32_t make_split(tpe_ctx* ctx, DevBuf& hi, DevBuf& lo, int32_t rows, int32_t c
 
 }  // namespace
 
-int32_t mixed_padded_size(int32_t V) {
-    int32_t vp = kT;
-    while (vp < V) vp *= 2;
-    return vp;
+int32_t mixed_padded_size(int32_t V) { return V <= kT ? kT : (V + kT - 1) / kT * kT; }
+
+namespace {
+// Rows of the first part of an uneven split of n rows (n a multiple of 128, at
+// least 256): the largest 128 * 2^k below n, so the first part's levels batch.
+int32_t first_part(int32_t n) {
+    int32_t h = kT;
+    while (2 * h < n) h *= 2;
+    return h;
 }
+bool pow2_blocks(int32_t n) { return n >= kT && ((n / kT) & (n / kT - 1)) == 0; }
+}  // namespace
 
 // FP32 factorization and inverse of the scaled A_rho (steps 1-3 above).
 // *ok = false when the FP32 factorization broke down.
@@ -767,6 +797,61 @@ int32_t inverse_half(tpe_ctx* ctx, int32_t base, int32_t hs, cudaStream_t s, int
     }
     return TPE_OK;
 }
+
+// Launches inverse_half issues for hs rows.
+int64_t inverse_half_launches(int32_t hs) {
+    int64_t n = 1;
+    for (int32_t m = kT; m < hs; m *= 2) n += 3;
+    return n;
+}
+
+// Launches inverse_rec issues for n rows.
+int64_t inverse_rec_launches(int32_t n) {
+    if (pow2_blocks(n)) return inverse_half_launches(n);
+    const int32_t a = first_part(n);
+    return inverse_half_launches(a) + inverse_rec_launches(n - a) + 3;
+}
+
+// Z = L^{-1} (and W = Z^T) on the rows [base, base + n), n any multiple of 128,
+// on stream s: a first part of 128 * 2^k rows by inverse_half, the rest
+// recursively, then the cross block Z21 = -Z22 (L21 Z11) through
+// T^T = W11 L21^T (T rows from base, free by then: every earlier use of T on
+// this stream inside [base, base + n) has finished, and the first part of the
+// top level, on another stream, uses only rows below base / 2).
+int32_t inverse_rec(tpe_ctx* ctx, int32_t base, int32_t n, cudaStream_t s, int32_t* d_err,
+                    int32_t* ctr) {
+    if (pow2_blocks(n)) return inverse_half(ctx, base, n, s, d_err, ctr);
+    MixedFactor& mf = ctx->mf;
+    const int32_t a = first_part(n), b = n - a;
+    // each inverse_half takes its own tile counters (two per level, at most 16)
+    TPE_TRY(inverse_half(ctx, base, a, s, d_err, ctr));
+    TPE_TRY(inverse_rec(ctx, base + a, b, s, d_err, ctr + 16));
+    tc::GemmArgs t;  // T^T (a x b) = W11 L21^T, W11 upper
+    t.a_r0 = t.a_c0 = base;
+    t.b_r0 = base + a;
+    t.b_c0 = base;
+    t.c_r0 = base;
+    t.M = a;
+    t.N = b;
+    t.K = a;
+    t.mode = tc::kAUpper;
+    TPE_CUDA_TRY(tc::gemm_nt(mf.W, mf.L, mf.T, t, d_err, s));
+    tc::GemmArgs u;  // Z21 (b x a) = -Z22 T, Z22 lower
+    u.a_r0 = u.a_c0 = base + a;
+    u.b_r0 = base;
+    u.c_r0 = base + a;
+    u.c_c0 = base;
+    u.M = b;
+    u.N = a;
+    u.K = b;
+    u.mode = tc::kALower;
+    u.alpha = -1.0f;
+    TPE_CUDA_TRY(tc::gemm_nt(mf.Z, mf.T, mf.Z, u, d_err, s));
+    transpose_rect_kernel<<<dim3(a / 32, b / 32, 1), dim3(32, 8), 0, s>>>(
+        mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, mf.Vp, base + a, base);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
 }  // namespace
 
 int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, bool* ok) {
@@ -785,9 +870,13 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     TPE_TRY(make_split(ctx, ctx->mx_Lhi, ctx->mx_Llo, Vp, Vp, mf.L));
     TPE_TRY(make_split(ctx, ctx->mx_Zhi, ctx->mx_Zlo, Vp, Vp, mf.Z));
     TPE_TRY(make_split(ctx, ctx->mx_Whi, ctx->mx_Wlo, Vp, Vp, mf.W));
+    // the top level's split: H1 = 128 * 2^k rows, the largest below Vp, then H2
+    const int32_t H1 = Vp > kT ? first_part(Vp) : Vp, H2 = Vp - H1;
     if (Vp > kT) {
-        TPE_TRY(make_split(ctx, ctx->mx_Thi, ctx->mx_Tlo, Vp / 2, Vp / 2, mf.T));
-        TPE_TRY(make_split(ctx, ctx->mx_T2hi, ctx->mx_T2lo, Vp / 2, Vp / 2, mf.T2));
+        // T: level scratch (inverse_half: rows base/2 ..) and the cross blocks of
+        // uneven splits (rows base ..); T2: the top level's T^T (H1 x H2)
+        TPE_TRY(make_split(ctx, ctx->mx_Thi, ctx->mx_Tlo, Vp, Vp / 2, mf.T));
+        TPE_TRY(make_split(ctx, ctx->mx_T2hi, ctx->mx_T2lo, H1, H2, mf.T2));
     }
     TPE_TRY(ensure(ctx, ctx->mx_Zd, sizeof(float) * (size_t)Vp * Vp));
     TPE_TRY(ensure(ctx, ctx->mx_Wd, sizeof(float) * (size_t)Vp * Vp));
@@ -807,7 +896,9 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     TPE_CUDA_TRY(cudaMemsetAsync(d_bad, 0, 2 * sizeof(int32_t), st));
     // tile counters of the persistent GEMMs: one per panel's trailing update,
     // then two per inverse level
-    const size_t nctr = (size_t)(Vp / kT) + 64;
+    // (nb for the trailing updates; 16 for the first part of the inverse, 16 per
+    // recursion depth of the rest, one for the top level)
+    const size_t nctr = (size_t)(Vp / kT) + 256;
     TPE_TRY(ensure(ctx, ctx->mx_ctr, sizeof(int32_t) * nctr));
     int32_t* d_ctr = ctx->mx_ctr.as<int32_t>();
     TPE_CUDA_TRY(cudaMemsetAsync(d_ctr, 0, sizeof(int32_t) * nctr, st));
@@ -858,10 +949,8 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     const int32_t rest_ctas = std::max(16, ctx->num_sms - ctx->grad_sms - 8);
     {
         const int64_t nrest = nb > 2 ? nb - 2 : 0;
-        int sub_h = 0;  // inverse levels of the first half (stream4, below)
-        for (int32_t m = kT; m < Vp / 2; m *= 2) sub_h++;
         KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + (int64_t)(nb - 1) + 4 * nrest + (nrest > 0 ? nrest - 1 : 0) +
-                                                     (nb > 1 ? 2 + 3 * (int64_t)sub_h : 0));
+                                                     (nb > 1 ? 1 + inverse_half_launches(H1) : 0));
         jacobi_kernel<<<nblk(Vp, 256), 256, 0, st>>>(d_A, V, Vp, shift, d, ctx->mx_dinv.as<double>());
         scale_to_f32_kernel<<<dim3((unsigned)((Vp + 1023) / 1024), (unsigned)std::min(Vp, 65535)), 256, 0,
                               st>>>(d_A, V, Vp, shift, d, S);
@@ -942,16 +1031,16 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
                     TC_TRY(tc::gemm_nt(mf.L, mf.L, Sm, u, d_err, st2, rest_ctas, d_ctr + j));
                 TPE_CUDA_TRY(cudaEventRecord(ev_r[j], st2));
             }
-            if (nb > 1 && j == nb / 2 - 1) {
-                // panels 0 .. nb/2-1 are final: the first half of the inverse and
+            if (nb > 1 && j == H1 / kT - 1) {
+                // panels 0 .. H1/128-1 are final: the first part of the inverse and
                 // the top level's T^T = W11 L21^T go to stream4 (low priority)
                 TPE_CUDA_TRY(cudaEventRecord(ev_mid, more ? st5 : st));
                 TPE_CUDA_TRY(cudaStreamWaitEvent(ctx->stream4, ev_mid, 0));
-                const int32_t H = Vp / 2;
-                TPE_TRY(inverse_half(ctx, 0, H, ctx->stream4, d_err, d_ctr + Vp / kT));
-                tc::GemmArgs t2;  // T^T (H x H) = W11 L21^T
-                t2.b_r0 = H;
-                t2.M = t2.N = t2.K = H;
+                TPE_TRY(inverse_half(ctx, 0, H1, ctx->stream4, d_err, d_ctr + Vp / kT));
+                tc::GemmArgs t2;  // T^T (H1 x H2) = W11 L21^T
+                t2.b_r0 = H1;
+                t2.M = t2.K = H1;
+                t2.N = H2;
                 t2.mode = tc::kAUpper;
                 TC_TRY(tc::gemm_nt(mf.W, mf.L, mf.T2, t2, d_err, ctx->stream4));
                 TPE_CUDA_TRY(cudaEventRecord(ev_half, ctx->stream4));
@@ -964,44 +1053,50 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
         TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_side, 0));
     }
     {
-        // Z = L^{-1} (W = Z^T alongside) by recursive halving. The first half
-        // (rows < Vp/2: its diagonal transposes, its levels and the top level's
-        // T^T = W11 L21^T) depends only on panels 0 .. nb/2-1, so it already ran
-        // on stream4 beside the second half of the factorization; the second half
-        // and the top level's Z21 = -Z22 T follow here.
-        int sub = 0;  // levels below the top one
-        for (int32_t m = kT; m < Vp / 2; m *= 2) sub++;
-        KernelScope ks(ctx, TPE_KGROUP_TRSV, Vp > kT ? 3 + 3 * (int64_t)sub : 1);
+        // Z = L^{-1} (W = Z^T alongside) by the recursive block formula. The
+        // first part (rows < H1: its diagonal transposes, its levels and the top
+        // level's T^T = W11 L21^T) depends only on panels 0 .. H1/128-1, so it
+        // already ran on stream4 beside the rest of the factorization; the rest
+        // (rows H1 ..) and the top level's Z21 = -Z22 T follow here.
         if (Vp == kT) {
+            KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
             diag_transpose_kernel<<<dim3(kT / 32, kT / 32, 1), dim3(32, 8), 0, st>>>(
                 mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, 0);
             TPE_CUDA_TRY(cudaGetLastError());
         } else {
-            const int32_t H = Vp / 2;
-            TPE_TRY(inverse_half(ctx, H, H, st, d_err, d_ctr + Vp / kT + 32));
+            KernelScope ks(ctx, TPE_KGROUP_TRSV, inverse_rec_launches(H2) + 2);
+            TPE_TRY(inverse_rec(ctx, H1, H2, st, d_err, d_ctr + Vp / kT + 32));
             TPE_CUDA_TRY(cudaStreamWaitEvent(st, ev_half, 0));
-            tc::GemmArgs u;  // top level: Z21 = -Z22 T
-            u.a_r0 = u.a_c0 = H;
-            u.c_r0 = H;
-            u.M = u.N = u.K = H;
+            tc::GemmArgs u;  // top level: Z21 (H2 x H1) = -Z22 T
+            u.a_r0 = u.a_c0 = H1;
+            u.c_r0 = H1;
+            u.M = u.K = H2;
+            u.N = H1;
             u.mode = tc::kALower;
             u.alpha = -1.0f;
             // no later product reads it split: written straight into the CG's FP32 copy
-            TC_TRY(tc::gemm_nt(mf.Z, mf.T2, mf.Zf, u, d_err, st, H >= 1024 ? ctx->num_sms : 0,
-                               d_ctr + Vp / kT + 63));
-            transpose_f32_kernel<<<dim3(H / 32, H / 32, 1), dim3(32, 8), 0, st>>>(
-                ctx->mx_Zd.as<float>(), ctx->mx_Wd.as<float>(), Vp, H, H);
+            TC_TRY(tc::gemm_nt(mf.Z, mf.T2, mf.Zf, u, d_err, st, H1 >= 1024 ? ctx->num_sms : 0,
+                               d_ctr + Vp / kT + 255));
+            transpose_f32_kernel<<<dim3(H1 / 32, H2 / 32, 1), dim3(32, 8), 0, st>>>(
+                ctx->mx_Zd.as<float>(), ctx->mx_Wd.as<float>(), Vp, H1);
             TPE_CUDA_TRY(cudaGetLastError());
         }
     }
     {
-        // the diagonal halves (the whole matrix when it is one block)
-        const int32_t nh = Vp > kT ? Vp / 2 : Vp;
-        KernelScope ks(ctx, TPE_KGROUP_TRSV, Vp / nh);
-        for (int32_t r0 = 0; r0 < Vp; r0 += nh)
-            factor_to_f32_kernel<<<nblk((int64_t)nh * nh, 256), 256, 0, st>>>(
-                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, r0, nh, ctx->mx_Zd.as<float>(),
+        // the diagonal parts (the whole matrix when it is one block)
+        KernelScope ks(ctx, TPE_KGROUP_TRSV, Vp > kT ? 2 : 1);
+        if (Vp > kT) {
+            factor_to_f32_kernel<<<nblk((int64_t)H1 * H1, 256), 256, 0, st>>>(
+                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, 0, H1, ctx->mx_Zd.as<float>(),
                 ctx->mx_Wd.as<float>());
+            factor_to_f32_kernel<<<nblk((int64_t)H2 * H2, 256), 256, 0, st>>>(
+                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, H1, H2, ctx->mx_Zd.as<float>(),
+                ctx->mx_Wd.as<float>());
+        } else {
+            factor_to_f32_kernel<<<nblk((int64_t)Vp * Vp, 256), 256, 0, st>>>(
+                mf.Z.hi, mf.Z.lo, mf.W.hi, mf.W.lo, Vp, 0, Vp, ctx->mx_Zd.as<float>(),
+                ctx->mx_Wd.as<float>());
+        }
         TPE_CUDA_TRY(cudaGetLastError());
     }
     int32_t flags[2] = {0, 0};

@@ -33,7 +33,9 @@ def _step(v, e, blocks, **opts):
     return T.sobolevStepSet(v, e, None, blocks, o)
 
 
-@pytest.mark.parametrize("V", [256, 1024, 2048])
+# 300, 2500 and 4097 are not multiples of 128 times a power of two: the factor
+# is padded to the next multiple of 128 and the inverse splits unevenly
+@pytest.mark.parametrize("V", [256, 300, 1024, 2048, 2500, 4097])
 def test_mixed_matches_fp64_step(V):
     v, e = F.random_walk_knot(V, seed=1)
     blocks = _set(v, e)
