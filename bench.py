@@ -588,12 +588,30 @@ def run_repulsive(args):
                 "taus": [x["tau"] for x in log], "cg_iterations": [x["refine"] for x in log],
                 "energy_last": log[-1]["energy"] if log else None}
 
-    # free-running: the two timed trajectories (b)
+    # free-running: the two timed trajectories (b), beside the FP64 trajectory
+    # from a start perturbed by 1e-12 relative (the descent map's own sensitivity)
     split = next((i for i, (a, b) in enumerate(zip(log_mix, log_64)) if a["tau"] != b["tau"]), None)
     traj_cmp = {"first_step_with_different_tau": split,
                 "energy_last_rel_diff": (abs(log_mix[-1]["energy"] - log_64[-1]["energy"]) / abs(log_64[-1]["energy"])
                                          if log_mix and log_64 else None),
                 "method": "the two timed trajectories, each step from its own previous output"}
+    if rank == 0:
+        rng = np.random.default_rng(0)
+        xp = v + 1e-12 * np.linalg.norm(v) / np.sqrt(v.size) * rng.standard_normal(v.shape)
+        ebp = T.calculateEnergy(xp, e)
+        taus_p = []
+        for _ in range(args.steps):
+            r = T.sobolevStepSet(xp, e, None, blocks, {"projectionMode": "frozen", "energyBefore": ebp,
+                                                       "precision": "fp64", "trials": 1})
+            taus_p.append(r["stats"]["tau"])
+            if r["accepted"]:
+                xp, ebp = r["vertices"], r["energy"]
+        traj_cmp["fp64_from_start_perturbed_1e-12"] = {
+            "taus": taus_p,
+            "first_step_with_different_tau": next((i for i, (a, b) in enumerate(zip(taus_p, log_64))
+                                                   if a != b["tau"]), None),
+            "note": "the FP64 step itself, from a start 1e-12 away: free-running trajectories separate "
+                    "after a few steps whatever the solve (a relative difference grows 10-100x per step)"}
 
     # Key order: the long blocks first, the metric's comparison last (the end of
     # the line is what a truncated log shows).

@@ -101,29 +101,46 @@ def test_gradient_along_trajectory_against_oracle(traj):
         assert rel(g, O.gradient(X[i], e)) <= 1e-10, i
 
 
-def test_fp64_free_running_trajectory(traj):
-    """20 GPU steps, each from the previous GPU output (the app's loop): the
-    same taus and projection iterations as the oracle's trajectory at every
-    step. The iterates drift apart slowly (each step adds its own ~1e-11
-    relative difference, and the descent map carries earlier ones along), so
-    the whole-trajectory bounds are looser than the per-step ones: vertices
-    1e-8, energies 1e-7 relative."""
-    X, e = traj["vertices"], traj["edges"]
-    blocks = _set(X[0])
-    x, eb = X[0].copy(), float(traj["energy"][0])
-    errs = []
-    for i in range(len(traj["tau"])):
+def _free_run(x0, e, blocks, n):
+    x, eb = x0.copy(), T.calculateEnergy(x0, e)
+    xs, taus, its = [x.copy()], [], []
+    for _ in range(n):
         r = T.sobolevStepSet(x, e, None, blocks, {"projectionMode": "frozen", "energyBefore": eb})
-        same = (r["stats"]["tau"] == traj["tau"][i] and
-                r["stats"]["projectionIterations"] == traj["projection_iterations"][i])
+        taus.append(r["stats"]["tau"])
+        its.append(r["stats"]["projectionIterations"])
         if r["accepted"]:
             x, eb = r["vertices"], r["energy"]
-        errs.append((i, same, rel(x, X[i + 1]), abs(eb - traj["energy"][i + 1]) / abs(traj["energy"][i + 1])))
-    print("free-running (step, same tau and iterations, vertices, energy):",
-          [(i, s_, f"{a:.2e}", f"{b:.2e}") for i, s_, a, b in errs])
-    assert all(s_ for _, s_, _, _ in errs)
-    assert max(a for _, _, a, _ in errs) <= 1e-8
-    assert max(b for _, _, _, b in errs) <= 1e-7
+        xs.append(x.copy())
+    return xs, taus, its
+
+
+def test_fp64_free_running_trajectory(traj):
+    """20 GPU steps, each from the previous GPU output (the app's loop), against
+    the oracle's trajectory. The descent map is very sensitive to its iterate:
+    a relative difference grows by one to two orders of magnitude per step
+    (a frozen Newton projection that converges in 5 iterations from one iterate
+    can need 30 from a neighbour 1e-3 away, which flips the accepted tau). So
+    the free-running comparison is held only over the first four steps (same
+    taus and projection iterations, iterates within 2e-9); the test then shows
+    the sensitivity itself: the same GPU trajectory from a start perturbed by
+    1e-12 relative leaves the unperturbed one by more than 1e-6 within 20
+    steps. Every single step is pinned by test_fp64_steps_against_oracle."""
+    X, e = traj["vertices"], traj["edges"]
+    blocks = _set(X[0])
+    n = len(traj["tau"])
+    xs, taus, its = _free_run(X[0], e, blocks, n)
+    errs = [rel(xs[i + 1], X[i + 1]) for i in range(n)]
+    print("free-running vs oracle, per step (same tau, iterate error):",
+          [(bool(taus[i] == traj["tau"][i]), f"{errs[i]:.1e}") for i in range(n)])
+    for i in range(4):
+        assert taus[i] == traj["tau"][i] and its[i] == traj["projection_iterations"][i], i
+        assert errs[i] <= 2e-9, (i, errs[i])
+    rng = np.random.default_rng(0)
+    x0p = X[0] + 1e-12 * np.linalg.norm(X[0]) / np.sqrt(X[0].size) * rng.standard_normal(X[0].shape)
+    xp, _, _ = _free_run(x0p, e, blocks, n)
+    drift = [rel(xp[i + 1], xs[i + 1]) for i in range(n)]
+    print("1e-12 perturbed start, drift per step:", [f"{d:.1e}" for d in drift])
+    assert max(drift) > 1e-6
 
 
 def test_mixed_steps_against_oracle(traj):
