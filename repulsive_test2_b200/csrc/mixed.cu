@@ -34,7 +34,6 @@ namespace tpe {
 namespace {
 
 constexpr int kT = 128;       // diagonal block = GEMM tile
-constexpr int kLd = kT + 1;   // shared-memory row stride of a block (floats)
 constexpr int kMaxRhs = 16;   // right-hand sides per CG pass
 
 __host__ __device__ __forceinline__ void split32(float x, float& hi, float& lo) {
@@ -104,10 +103,26 @@ __global__ void split_copy_kernel(const float* __restrict__ S, int32_t ld, int32
     lo[o] = l;
 }
 
-constexpr int kPw = 32;        // panel width inside a diagonal block
-constexpr int kPl = kPw + 1;   // row stride of the panel scratch
+constexpr int kLd3 = 132;   // row stride of a and z (16-byte aligned rows)
+constexpr int kP3 = 100;    // row stride of plT (the panel, transposed)
+constexpr int kS3 = 36;     // row stride of the 32 x 32 scratch blocks
+constexpr int kTs3 = 36;    // row stride of the off-diagonal T scratch
+constexpr int kPw3 = 32;
 
-// Decodes the packed lower-triangular index e into (ti, tj), tj <= ti.
+// shared-memory offsets (floats)
+constexpr int kOffA = 0;
+constexpr int kOffZ = kOffA + kT * kLd3;
+constexpr int kOffP = kOffZ + kT * kLd3;               // plT: 32 x kP3, also the final T scratch
+constexpr int kPSize = 3 * 32 * kTs3 > 32 * kP3 ? 3 * 32 * kTs3 : 32 * kP3;
+constexpr int kOffTsc = kOffP + kPSize;               // 2 x 32 x kTs3
+constexpr int kOffRd = kOffTsc + 2 * 32 * kTs3;       // 128
+constexpr int kOffZdT = kOffRd + kT;                  // 32 x kS3: Z_dd^T of the current panel
+constexpr int kOffLt = kOffZdT + 32 * kS3;            // 32 x kS3: L_dd^T (wf32 scratch)
+constexpr int kOffC4 = kOffLt + 32 * kS3;             // 32 float4 (wf32 scratch)
+constexpr int kSmem3Floats = kOffC4 + 128;
+static_assert(kOffZ % 4 == 0 && kOffP % 4 == 0 && kOffTsc % 4 == 0 && kOffZdT % 4 == 0 &&
+              kOffLt % 4 == 0 && kOffC4 % 4 == 0, "float4 alignment");
+
 __device__ __forceinline__ void tri_decode(int e, int& ti, int& tj) {
     int t = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
     while ((t + 1) * (t + 2) / 2 <= e) t++;
@@ -116,92 +131,214 @@ __device__ __forceinline__ void tri_decode(int e, int& ti, int& tj) {
     tj = e - t * (t + 1) / 2;
 }
 
-// Column K of the in-register Cholesky of a 32 x 32 block (lane = row):
-// pivot from lane K, scale column K, update the columns right of it; the
-// template recursion keeps every register index static.
-template <int K>
-__device__ __forceinline__ void chol_col(float (&v)[32], int lane, bool& brk, float& myrs) {
-    if constexpr (K < 32) {
-        float piv = __shfl_sync(0xffffffffu, v[K], K);
-        if (!(piv > 0.0f) || !isfinite(piv)) {
-            brk = true;
-            piv = 1.0f;
-        }
-        const float rs = rsqrtf(piv);
-        if (lane == K) {
-            v[K] = piv * rs;
-            myrs = rs;
-        } else {
-            v[K] *= rs;
-        }
-        const float lk = v[K];
-#pragma unroll
-        for (int m = K + 1; m < 32; m++) {
-            const float lmk = __shfl_sync(0xffffffffu, v[K], m);
-            if (lane >= m) v[m] -= lk * lmk;
-        }
-        chol_col<K + 1>(v, lane, brk, myrs);
-    }
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float f4(const float4& v, int i) {
+    return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
 }
 
-// Warp-level factor of the 32 x 32 diagonal part of panel c0 (lane = row,
-// column values shared by shuffles, no block barriers), then its inverse by
-// forward substitution (lane = column of the inverse) into z, 1/L_ii into rd.
-// Not inlined: the unrolled body is long, and a single copy shared by the
-// four panels is fetched into the instruction cache once per launch instead of
-// once per call site.
-__device__ __noinline__ void warp_factor32(float* a, float* z, float* rd, int c0, int lane,
-                                              int32_t* bad) {
-    float v[kPw];
+// One warp factors the 32 x 32 diagonal part at (c0, c0) of a (lane = row) and
+// inverts it. Columns in groups of four: inside a group the rank-1 updates use
+// shuffles; the group's four columns then go to shared memory once (one
+// float4 per row) and the later columns take a rank-4 update from 16-byte
+// loads. The inverse (lane = column of Z) reads L column-wise from a
+// transposed copy. Writes L to a, Z (lower) to z, Z^T to zdt, 1/L_ii to rd.
+__device__ __noinline__ void warp_factor32(float* sm, int c0, int lane, int32_t* bad) {
+    float* a = sm + kOffA;
+    float* z = sm + kOffZ;
+    float* rd = sm + kOffRd;
+    float* zdt = sm + kOffZdT;
+    float* lt = sm + kOffLt;
+    float4* c4 = reinterpret_cast<float4*>(sm + kOffC4);
+    float v[32];
 #pragma unroll
-    for (int m = 0; m < kPw; m++) v[m] = (m <= lane) ? a[(c0 + lane) * kLd + c0 + m] : 0.0f;
+    for (int q = 0; q < 8; q++) {
+        const float4 x = ld4(a + (c0 + lane) * kLd3 + c0 + 4 * q);
+        v[4 * q] = (4 * q <= lane) ? x.x : 0.0f;
+        v[4 * q + 1] = (4 * q + 1 <= lane) ? x.y : 0.0f;
+        v[4 * q + 2] = (4 * q + 2 <= lane) ? x.z : 0.0f;
+        v[4 * q + 3] = (4 * q + 3 <= lane) ? x.w : 0.0f;
+    }
     bool brk = false;
     float myrs = 1.0f;
-    chol_col<0>(v, lane, brk, myrs);
-    if (brk && lane == 0) atomicExch(bad, 1);
 #pragma unroll
-    for (int m = 0; m < kPw; m++) a[(c0 + lane) * kLd + c0 + m] = (m <= lane) ? v[m] : 0.0f;
+    for (int g = 0; g < 8; g++) {
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            const int K = 4 * g + kk;
+            float piv = __shfl_sync(0xffffffffu, v[K], K);
+            if (!(piv > 0.0f) || !isfinite(piv)) {
+                brk = true;
+                piv = 1.0f;
+            }
+            const float rs = rsqrtf(piv);
+            const float lk = (lane == K) ? piv * rs : v[K] * rs;
+            if (lane >= K) v[K] = lk;
+            if (lane == K) myrs = rs;
+#pragma unroll
+            for (int m = K + 1; m < 4 * g + 4; m++) {
+                const float lmk = __shfl_sync(0xffffffffu, lk, m);
+                if (lane >= m) v[m] = fmaf(-lk, lmk, v[m]);
+            }
+        }
+        if (g < 7) {
+            c4[lane] = make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
+            __syncwarp();
+#pragma unroll
+            for (int m = 4 * g + 4; m < 32; m++) {
+                const float4 q = c4[m];
+                if (lane >= m) {
+                    float t = v[m];
+                    t = fmaf(-v[4 * g], q.x, t);
+                    t = fmaf(-v[4 * g + 1], q.y, t);
+                    t = fmaf(-v[4 * g + 2], q.z, t);
+                    t = fmaf(-v[4 * g + 3], q.w, t);
+                    v[m] = t;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (brk && lane == 0) atomicExch(bad, 1);
+    // L back to a (rows, 16-byte stores), L^T to lt (lt[k][lane] = L[lane][k]), 1/L_ii
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+        st4(a + (c0 + lane) * kLd3 + c0 + 4 * q, make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
+#pragma unroll
+    for (int k = 0; k < 32; k++) lt[k * kS3 + lane] = v[k];
     rd[c0 + lane] = myrs;
     __syncwarp();
-    float x[kPw];
+    // inverse, lane = column j: x[i] = Z[i][j]
+    float x[32];
 #pragma unroll
-    for (int i = 0; i < kPw; i++) x[i] = (i == lane) ? 1.0f : 0.0f;
+    for (int i = 0; i < 32; i++) x[i] = (i == lane) ? 1.0f : 0.0f;
+    float rdv[32];
 #pragma unroll
-    for (int k = 0; k < kPw; k++) {
-        x[k] *= rd[c0 + k];
-#pragma unroll
-        for (int i = k + 1; i < kPw; i++) x[i] -= a[(c0 + i) * kLd + c0 + k] * x[k];
+    for (int q = 0; q < 8; q++) {
+        const float4 r4 = ld4(rd + c0 + 4 * q);
+        rdv[4 * q] = r4.x;
+        rdv[4 * q + 1] = r4.y;
+        rdv[4 * q + 2] = r4.z;
+        rdv[4 * q + 3] = r4.w;
     }
 #pragma unroll
-    for (int i = 0; i < kPw; i++) z[(c0 + i) * kLd + c0 + lane] = (i >= lane) ? x[i] : 0.0f;
+    for (int k = 0; k < 32; k++) {
+        x[k] *= rdv[k];
+#pragma unroll
+        for (int q = (k + 1) / 4; q < 8; q++) {
+            const float4 l4 = ld4(lt + k * kS3 + 4 * q);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = 4 * q + u;
+                if (i > k) x[i] = fmaf(-f4(l4, u), x[k], x[i]);
+            }
+        }
+    }
+    // Z rows to z (column lane), Z^T rows to zdt (row lane)
+#pragma unroll
+    for (int i = 0; i < 32; i++) z[(c0 + i) * kLd3 + c0 + lane] = (i >= lane) ? x[i] : 0.0f;
+#pragma unroll
+    for (int q = 0; q < 8; q++)
+        st4(zdt + lane * kS3 + 4 * q,
+            make_float4(4 * q >= lane ? x[4 * q] : 0.0f, 4 * q + 1 >= lane ? x[4 * q + 1] : 0.0f,
+                        4 * q + 2 >= lane ? x[4 * q + 2] : 0.0f, 4 * q + 3 >= lane ? x[4 * q + 3] : 0.0f));
     __syncwarp();
 }
 
-// a[R..R+3][C..C+3] -= pl[4ti..][.] pl[4tj..][.]^T over the 32 panel columns.
-__device__ __forceinline__ void update_tile(float* a, const float* pl, int ti, int tj, int base) {
+// a[R..R+3][C..C+3] -= P rows (4ti..) P rows (4tj..)^T over the 32 panel columns
+// (P transposed in plT).
+__device__ __forceinline__ void update_tile(float* a, const float* plt, int ti, int tj, int base) {
     float acc[4][4];
 #pragma unroll
     for (int x = 0; x < 4; x++)
 #pragma unroll
         for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
-#pragma unroll 4
-    for (int k = 0; k < kPw; k++) {
-        float pr[4], pc[4];
-#pragma unroll
-        for (int x = 0; x < 4; x++) {
-            pr[x] = pl[(4 * ti + x) * kPl + k];
-            pc[x] = pl[(4 * tj + x) * kPl + k];
-        }
+#pragma unroll 8
+    for (int k = 0; k < kPw3; k++) {
+        const float4 pr = ld4(plt + k * kP3 + 4 * ti);
+        const float4 pc = ld4(plt + k * kP3 + 4 * tj);
 #pragma unroll
         for (int x = 0; x < 4; x++)
 #pragma unroll
-            for (int y = 0; y < 4; y++) acc[x][y] += pr[x] * pc[y];
+            for (int y = 0; y < 4; y++) acc[x][y] += f4(pr, x) * f4(pc, y);
     }
     const int R = base + 4 * ti, Cc = base + 4 * tj;
 #pragma unroll
+    for (int x = 0; x < 4; x++) {
+        float* p = a + (R + x) * kLd3 + Cc;
+        float4 o = ld4(p);
+        o.x -= acc[x][0];
+        o.y -= acc[x][1];
+        o.z -= acc[x][2];
+        o.w -= acc[x][3];
+        st4(p, o);
+    }
+}
+
+__device__ __forceinline__ void group_sync(int bar, int nthr) {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthr) : "memory");
+}
+
+// Off-diagonal 32 x 32 blocks of Z inside the block: for each listed pair
+// (bi, bj), bj < bi, T = sum_{c=bj}^{bi-1} L_{bi,c} Z_{c,bj}, then
+// Z_{bi,bj} = -Z_{bi,bi} T. 64 threads per pair (8 x 8 threads of 4 x 4 outputs).
+__device__ void offdiag_blocks(const float* __restrict__ a, float* __restrict__ z,
+                                float* __restrict__ tsc, const int* pa, const int* pb, int npairs,
+                                int t, int nthr, int bar) {
+    const int slot = t >> 6;
+    const bool act = slot < npairs;
+    const int tr = (t >> 3) & 7, tc = t & 7;
+    const int bi = act ? pa[slot] : 0, bj = act ? pb[slot] : 0;
+    float acc[4][4];
+#pragma unroll
     for (int x = 0; x < 4; x++)
 #pragma unroll
-        for (int y = 0; y < 4; y++) a[(R + x) * kLd + Cc + y] -= acc[x][y];
+        for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+    if (act) {
+        for (int k4 = bj * kPw3; k4 < bi * kPw3; k4 += 4) {
+            float4 lr[4], zc[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) lr[x] = ld4(a + (bi * kPw3 + 4 * tr + x) * kLd3 + k4);
+#pragma unroll
+            for (int u = 0; u < 4; u++) zc[u] = ld4(z + (k4 + u) * kLd3 + bj * kPw3 + 4 * tc);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+#pragma unroll
+                    for (int y = 0; y < 4; y++) acc[x][y] += f4(lr[x], u) * f4(zc[u], y);
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+            st4(tsc + (slot * kPw3 + 4 * tr + x) * kTs3 + 4 * tc,
+                make_float4(acc[x][0], acc[x][1], acc[x][2], acc[x][3]));
+    }
+    group_sync(bar, nthr);
+    if (act) {
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
+        const int qmax = 4 * tr + 4;  // Z_aa is lower: columns q <= row
+        for (int q4 = 0; q4 < qmax; q4 += 4) {
+            float4 zr[4], tq[4];
+#pragma unroll
+            for (int x = 0; x < 4; x++) zr[x] = ld4(z + (bi * kPw3 + 4 * tr + x) * kLd3 + bi * kPw3 + q4);
+#pragma unroll
+            for (int u = 0; u < 4; u++) tq[u] = ld4(tsc + (slot * kPw3 + q4 + u) * kTs3 + 4 * tc);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+#pragma unroll
+                    for (int y = 0; y < 4; y++) acc[x][y] += f4(zr[x], u) * f4(tq[u], y);
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+            st4(z + (bi * kPw3 + 4 * tr + x) * kLd3 + bj * kPw3 + 4 * tc,
+                make_float4(-acc[x][0], -acc[x][1], -acc[x][2], -acc[x][3]));
+    }
+    group_sync(bar, nthr);
 }
 
 // One CTA factors the 128 x 128 diagonal block at (j0, j0) of S (its lower
@@ -213,92 +350,26 @@ __device__ __forceinline__ void update_tile(float* a, const float* pl, int ti, i
 // Blocked right-looking over four 32-column panels with an in-CTA look-ahead:
 // warp 0 factors a panel's 32 x 32 diagonal part in registers and inverts it
 // (warp_factor32); all eight warps solve the rows below against that inverse
-// (warp = 4 columns, lane = row); then warp 0 alone applies the rank-32 update
-// to the next panel's diagonal part and factors it, while warps 1-7 update
-// the rest of the trailing triangle (4 x 4 register tiles). The off-diagonal
-// 32 x 32 blocks of the inverse follow from Z_ab = -Z_aa sum_{b<=c<a} L_ac Z_cb,
-// one block distance at a time. Reciprocal square roots are the fast
-// approximate ones: the factor is a preconditioner, CG restores FP64 accuracy.
-// *bad = 1 when a pivot is not positive and finite.
-// Off-diagonal 32 x 32 blocks of Z = L^{-1} inside a diagonal block: for each
-// listed pair (a, b), b < a, T = sum_{c=b}^{a-1} L_ac Z_cb, then Z_ab = -Z_aa T
-// (Z_aa lower). 64 threads per pair (8 x 8 threads of 4 x 4 outputs); threads
-// t < nthr of the caller's group, which synchronises on named barrier bar; tsc
-// holds 32 rows (stride kPl) of T per pair.
-__device__ __forceinline__ void group_sync(int bar, int nthr) {
-    asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nthr) : "memory");
-}
-
-__device__ void offdiag_blocks(const float* __restrict__ a, float* __restrict__ z,
-                               float* __restrict__ tsc, const int* pa, const int* pb, int npairs,
-                               int t, int nthr, int bar) {
-    const int slot = t >> 6;
-    const bool act = slot < npairs;
-    const int tr = (t >> 3) & 7, tc = t & 7;
-    const int bi = act ? pa[slot] : 0, bj = act ? pb[slot] : 0;
-    float acc[4][4];
-#pragma unroll
-    for (int x = 0; x < 4; x++)
-#pragma unroll
-        for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
-    if (act) {
-        for (int k = bj * kPw; k < bi * kPw; k++) {
-            float lr[4], zc[4];
-#pragma unroll
-            for (int x = 0; x < 4; x++) {
-                lr[x] = a[(bi * kPw + 4 * tr + x) * kLd + k];
-                zc[x] = z[k * kLd + bj * kPw + 4 * tc + x];
-            }
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) acc[x][y] += lr[x] * zc[y];
-        }
-#pragma unroll
-        for (int x = 0; x < 4; x++)
-#pragma unroll
-            for (int y = 0; y < 4; y++) tsc[(slot * kPw + 4 * tr + x) * kPl + 4 * tc + y] = acc[x][y];
-    }
-    group_sync(bar, nthr);
-    if (act) {
-#pragma unroll
-        for (int x = 0; x < 4; x++)
-#pragma unroll
-            for (int y = 0; y < 4; y++) acc[x][y] = 0.0f;
-        const int rmax = 4 * tr + 3;
-        for (int q = 0; q <= rmax; q++) {
-            float zr[4], tq[4];
-#pragma unroll
-            for (int x = 0; x < 4; x++) {
-                zr[x] = z[(bi * kPw + 4 * tr + x) * kLd + bi * kPw + q];
-                tq[x] = tsc[(slot * kPw + q) * kPl + 4 * tc + x];
-            }
-#pragma unroll
-            for (int x = 0; x < 4; x++)
-#pragma unroll
-                for (int y = 0; y < 4; y++) acc[x][y] += zr[x] * tq[y];
-        }
-#pragma unroll
-        for (int x = 0; x < 4; x++)
-#pragma unroll
-            for (int y = 0; y < 4; y++)
-                z[(bi * kPw + 4 * tr + x) * kLd + bj * kPw + 4 * tc + y] = -acc[x][y];
-    }
-    group_sync(bar, nthr);
-}
-
-__global__ void __launch_bounds__(256, 2)
+// (warp = 4 columns, lane = row, the panel stored transposed); then warps 0
+// and 1 apply the rank-32 update to the next panel's diagonal part and warp 0
+// factors it, while warps 1-7 update the rest of the trailing triangle (4 x 4
+// register tiles from 16-byte loads) and form the off-diagonal 32 x 32 blocks
+// of the inverse, Z_ab = -Z_aa sum_{b<=c<a} L_ac Z_cb, one block distance at a
+// time. Reciprocal square roots are the fast approximate ones: the factor is a
+// preconditioner, CG restores FP64 accuracy. *bad = 1 when a pivot is not
+// positive and finite. Rows of a and z are 132 floats apart (16-byte aligned),
+// so every shared-memory access of the inner loops is a 16-byte one.
+__global__ void __launch_bounds__(256, 1)
 potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __restrict__ Zhi,
-                float* __restrict__ Zlo, int32_t* __restrict__ bad) {
-    extern __shared__ float sm[];
-    float* a = sm;                  // the block, then L (lower; the upper part is never read)
-    float* z = a + kT * kLd;        // L^{-1} (lower)
-    float* pl = z + kT * kLd;       // 96 x 33 panel rows / block products
-    float* rd = pl + 96 * kPl;      // 1 / L_ii
-    float* tsc = rd + kT;           // 2 x 32 x 33: T of the off-diagonal blocks done in the loop
+            float* __restrict__ Zlo, int32_t* __restrict__ bad) {
+    extern __shared__ __align__(16) float sm[];
+    float* a = sm + kOffA;
+    float* z = sm + kOffZ;
+    float* plt = sm + kOffP;
+    float* zdt = sm + kOffZdT;
+    float* tsc = sm + kOffTsc;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     {
-        // whole block, 16-byte loads (ld and j0 are multiples of 128)
         float4 buf[16];
 #pragma unroll
         for (int q = 0; q < 16; q++) {
@@ -310,62 +381,69 @@ potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __re
         for (int q = 0; q < 16; q++) {
             const int e = tid + 256 * q;
             const int r = e >> 5, c = (e & 31) * 4;
-            a[r * kLd + c] = buf[q].x;
-            a[r * kLd + c + 1] = buf[q].y;
-            a[r * kLd + c + 2] = buf[q].z;
-            a[r * kLd + c + 3] = buf[q].w;
+            st4(a + r * kLd3 + c, buf[q]);
         }
     }
     __syncthreads();
-    if (warp == 0) warp_factor32(a, z, rd, 0, lane, bad);
+    if (warp == 0) warp_factor32(sm, 0, lane, bad);
     __syncthreads();
-    for (int p = 0; p < kT / kPw - 1; p++) {
-        const int c0 = p * kPw;
-        const int nr = kT - c0 - kPw;
-        // panel rows below: pl[r][m] = sum_k A[c0+32+r][c0+k] * Zd[m][k]
+    for (int p = 0; p < kT / kPw3 - 1; p++) {
+        const int c0 = p * kPw3;
+        const int nr = kT - c0 - kPw3;
+        // panel rows below: plT[m][r] = sum_k A[c0+32+r][c0+k] * Zd[m][k]
         {
             const int m0 = 4 * warp;
             for (int r0 = 0; r0 < nr; r0 += 32) {
                 const int r = r0 + lane;
-                const float* arow = a + (c0 + kPw + r) * kLd + c0;
+                const float* arow = a + (c0 + kPw3 + r) * kLd3 + c0;
                 float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll 8
-                for (int k = 0; k < kPw; k++) {
-                    const float ak = arow[k];
 #pragma unroll
-                    for (int t = 0; t < 4; t++) acc[t] += ak * z[(c0 + m0 + t) * kLd + c0 + k];
+                for (int k4 = 0; k4 < kPw3; k4 += 4) {
+                    const float4 ak = ld4(arow + k4);
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const float4 zk = ld4(zdt + (k4 + u) * kS3 + m0);
+                        const float av = f4(ak, u);
+                        acc[0] += av * zk.x;
+                        acc[1] += av * zk.y;
+                        acc[2] += av * zk.z;
+                        acc[3] += av * zk.w;
+                    }
                 }
 #pragma unroll
-                for (int t = 0; t < 4; t++) pl[r * kPl + m0 + t] = acc[t];
+                for (int t = 0; t < 4; t++) plt[(m0 + t) * kP3 + r] = acc[t];
             }
         }
         __syncthreads();
-        const int base = c0 + kPw;
+            const int base = c0 + kPw3;
         const int nt = nr / 4;
         const int ntiles = nt * (nt + 1) / 2;
         constexpr int kNext = 36;  // 4 x 4 tiles of the next 32 x 32 diagonal part (packed first)
-        if (warp == 0) {
-            for (int e = lane; e < kNext; e += 32) {
+        if (warp < 2) {
+            // warps 0 and 1: the next diagonal part, then warp 0 factors it
+            const int e = warp * 18 + lane;
+            if (lane < 18) {
                 int ti, tj;
                 tri_decode(e, ti, tj);
-                update_tile(a, pl, ti, tj, base);
+                update_tile(a, plt, ti, tj, base);
             }
-            __syncwarp();
-            warp_factor32(a, z, rd, base, lane, bad);
+            group_sync(3, 64);
+        }
+        if (warp == 0) {
+            warp_factor32(sm, base, lane, bad);
         } else {
             for (int e = kNext + tid - 32; e < ntiles; e += 224) {
                 int ti, tj;
                 tri_decode(e, ti, tj);
-                update_tile(a, pl, ti, tj, base);
+                update_tile(a, plt, ti, tj, base);
             }
             // the panel rows become final L
-            for (int e = tid - 32; e < nr * kPw; e += 224) {
+            for (int e = tid - 32; e < nr * kPw3; e += 224) {
                 const int r = e >> 5, m = e & 31;
-                a[(base + r) * kLd + c0 + m] = pl[r * kPl + m];
+                a[(base + r) * kLd3 + c0 + m] = plt[m * kP3 + r];
             }
             // while warp 0 factors the next panel: the off-diagonal Z blocks of
-            // block row p, whose inputs (L columns < 32 p, Z blocks of rows
-            // <= p) are final
+            // block row p (inputs final: L columns < 32 p, Z blocks of rows <= p)
             if (p > 0) {
                 int pa[2], pb[2];
                 for (int q = 0; q < p; q++) {
@@ -376,21 +454,26 @@ potrf128_kernel(const float* __restrict__ S, int32_t ld, int32_t j0, float* __re
             }
         }
         __syncthreads();
-    }
+        }
     // the last block row of Z: its three off-diagonal blocks at once
     {
         const int pa[3] = {3, 3, 3}, pb[3] = {2, 1, 0};
-        offdiag_blocks(a, z, pl, pa, pb, 3, tid, 256, 2);
+        offdiag_blocks(a, z, plt, pa, pb, 3, tid, 256, 2);
     }
-    // Z_jj (split): lane = column, coalesced rows
-    for (int e = tid; e < kT * kT; e += 256) {
-        const int r = e >> 7, c = e & (kT - 1);
+    // Z_jj (split), four columns per thread step, zero above the diagonal
+    for (int e = tid; e < kT * kT / 4; e += 256) {
+        const int r = e >> 5, c = (e & 31) * 4;
+        const float4 zz = ld4(z + r * kLd3 + c);
+        float4 h, l;
+        split32(c <= r ? zz.x : 0.0f, h.x, l.x);
+        split32(c + 1 <= r ? zz.y : 0.0f, h.y, l.y);
+        split32(c + 2 <= r ? zz.z : 0.0f, h.z, l.z);
+        split32(c + 3 <= r ? zz.w : 0.0f, h.w, l.w);
         const size_t o = (size_t)(j0 + r) * ld + j0 + c;
-        float h, l;
-        split32(c <= r ? z[r * kLd + c] : 0.0f, h, l);
-        Zhi[o] = h;
-        Zlo[o] = l;
+        *reinterpret_cast<float4*>(Zhi + o) = h;
+        *reinterpret_cast<float4*>(Zlo + o) = l;
     }
+    __syncthreads();
 }
 
 // W_jj = Z_jj^T for the diagonal blocks b0 + blockIdx.z, split.
@@ -917,7 +1000,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
         }
     }
     const int nb = Vp / kT;
-    const size_t potrf_smem = sizeof(float) * (2 * kT * kLd + 96 * kPl + kT + 2 * kPw * kPl);
+    const size_t potrf_smem = sizeof(float) * kSmem3Floats;
     TPE_CUDA_TRY(cudaFuncSetAttribute(potrf128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)potrf_smem));
     // Critical path on the main stream, per block j: potrf, then one CTA that
