@@ -25,12 +25,32 @@ namespace tpe {
 namespace {
 
 
-// (|d|+eps)^(-(2 sigma + 1)); MODE 1: alpha = 3, beta = 6 -> exponent 7/3.
+// (|d|+eps)^(-(2 sigma + 1)) from dn = |d|+eps and its reciprocal idn;
+// MODE 1: alpha = 3, beta = 6 -> exponent 7/3.
 template <int MODE>
-__device__ __forceinline__ double inv_dist_pow(double dn, double distExp) {
-    if (MODE == 1) return rcbrt(dn) / (dn * dn);
+__device__ __forceinline__ double inv_dist_pow(double dn, double idn, double distExp) {
+    if (MODE == 1) return rcbrt(dn) * (idn * idn);
     return 1.0 / pow(dn, distExp);
 }
+
+// |d| and 1/(|d| + eps) for x = |d|^2 from one reciprocal square root r:
+// 1/(|d| + eps) = r / (1 + t), t = eps r, summed as r (1 - t + t^2) when
+// t < 2^-20 (the first term left out is below 2^-60 relative); otherwise the
+// square root and the division themselves.
+__device__ __forceinline__ void dist_inv(double x, double eps, double& s, double& inv_se) {
+    const double r = rsqrt(x);
+    const double t = eps * r;
+    if (t < 9.5367431640625e-07) {
+        s = x * r;
+        inv_se = fma(-r, t * (1.0 - t), r);
+    } else {
+        s = sqrt(x);
+        inv_se = 1.0 / (s + eps);
+    }
+}
+
+// sqrt(x) for x >= 0 from a reciprocal square root (0 at x = 0).
+__device__ __forceinline__ double sqrt_r(double x) { return x > 0.0 ? x * rsqrt(x) : sqrt(x); }
 
 constexpr int kT = 32;  // pair tile: 32 edges I x 32 edges J
 
@@ -76,19 +96,21 @@ __device__ __forceinline__ double2 pair_weight(const EdgeRec& a, const EdgeRec& 
         const double dx = (ai ? a.p2.x : a.p1.x) - (bj ? b.p2.x : b.p1.x);
         const double dy = (ai ? a.p2.y : a.p1.y) - (bj ? b.p2.y : b.p1.y);
         const double dz = (ai ? a.p2.z : a.p1.z) - (bj ? b.p2.z : b.p1.z);
-        const double dn = sqrt(dx * dx + dy * dy + dz * dz) + eps;
-        const double kd = inv_dist_pow<MODE>(dn, distExp);
+        double dlen, idn;
+        dist_inv(dx * dx + dy * dy + dz * dz, eps, dlen, idn);
+        const double dn = dlen + eps;
+        const double kd = inv_dist_pow<MODE>(dn, idn, distExp);
         sumDist += kd;
-        const double dn2 = dn * dn;
-        const double kq = kd / (dn2 * dn2);
+        const double idn2 = idn * idn;
+        const double kq = kd * (idn2 * idn2);
         double cx = a.T.y * dz - a.T.z * dy, cy = a.T.z * dx - a.T.x * dz,
                cz = a.T.x * dy - a.T.y * dx;
-        double cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
+        double cn = sqrt_r(cx * cx + cy * cy + cz * cz) + eps;
         sumLowIJ += cn * cn * kq;
         cx = b.T.y * dz - b.T.z * dy;
         cy = b.T.z * dx - b.T.x * dz;
         cz = b.T.x * dy - b.T.y * dx;
-        cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
+        cn = sqrt_r(cx * cx + cy * cy + cz * cz) + eps;
         sumLowJI += cn * cn * kq;
     }
     const double ll = a.p1.w * b.p1.w;

@@ -538,25 +538,39 @@ __global__ void transpose_rect_kernel(const float* __restrict__ zhi, const float
 
 // ---- block CG kernels (vectors are [nr][Vp] FP64, pad entries stay 0) ------
 
-// U = D P, s[c] = sum_j U[c][j]   (one block per column)
-__global__ void cg_prep_kernel(const double* __restrict__ P, const double* __restrict__ d,
-                               int32_t V, int32_t Vp, double* __restrict__ U,
-                               double* __restrict__ s) {
-    __shared__ double red[8];
-    const int c = blockIdx.x;
-    double acc = 0.0;
-    for (int32_t j = threadIdx.x; j < V; j += blockDim.x) {
-        const double u = d[j] * P[(size_t)c * Vp + j];
-        U[(size_t)c * Vp + j] = u;
-        acc += u;
+
+// UT[j][c] = d_j P[c][j] for j < V, c < nr (0 elsewhere, up to Vp rows of 16),
+// and the column sums of each 256-row block into spart[block][c] (summed in a
+// fixed order by mrhs_t_reduce_kernel): the matvec's scaling and the sums its
+// rank-one shift needs, in right-hand-side-major form.
+__global__ void __launch_bounds__(256) cg_prep_t_kernel(const double* __restrict__ P,
+                                                       const double* __restrict__ d, int32_t V,
+                                                       int32_t Vp, int32_t nr,
+                                                       double* __restrict__ UT,
+                                                       double* __restrict__ spart) {
+    __shared__ double red[8][kMaxRhs];
+    const int32_t j = blockIdx.x * 256 + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double dj = j < V ? d[j] : 0.0;
+    double u[kMaxRhs];
+#pragma unroll
+    for (int c = 0; c < kMaxRhs; c++) u[c] = (c < nr && j < V) ? dj * P[(size_t)c * Vp + j] : 0.0;
+    if (j < Vp) {
+        double2* row = reinterpret_cast<double2*>(UT + (size_t)j * kMaxRhs);
+#pragma unroll
+        for (int c = 0; c < kMaxRhs; c += 2) row[c / 2] = make_double2(u[c], u[c + 1]);
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+#pragma unroll
+    for (int c = 0; c < kMaxRhs; c++) {
+        double v = u[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][c] = v;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < kMaxRhs) {
         double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
-        s[c] = t;
+        for (int w = 0; w < 8; w++) t += red[w][threadIdx.x];
+        spart[(size_t)blockIdx.x * kMaxRhs + threadIdx.x] = t;
     }
 }
 
@@ -660,6 +674,156 @@ mrhs_dmma_kernel(const MT* __restrict__ M, int32_t ldm, int32_t n,
         P[(size_t)(8 + cb) * ldx + row] = c1a;
         P[(size_t)(9 + cb) * ldx + row] = c1b;
     }
+}
+
+// ---- the CG's multi-RHS products, right-hand-side-major form ------------------
+//
+// Y = M X for up to 16 right-hand sides with the vectors held right-hand-side
+// major (XT[j][c], 16 doubles per row j): every DMMA B fragment is then eight
+// consecutive doubles of four rows (256 bytes in 8 sectors) read straight from
+// L2, with no shared-memory staging and no block barriers. A warp owns 32 rows
+// (four m8 fragments sharing each B fragment), a CTA 128 rows (one 128-row tile
+// of the FP32 factor copies, whose lower or upper tiles alone are defined), and
+// the columns split into chunks of kKChunk (grid.x) whose partial sums go to
+// part[chunk][c][row] for a fixed-order reduction.
+constexpr int kKChunk = 512;
+constexpr int kTRows = 128;   // rows per CTA (four warps of 32)
+
+// XT[j][c] = X[c][j] (j < n, c < nr), 0 elsewhere; nout rows of 16.
+__global__ void rhs_major_kernel(const double* __restrict__ X, int32_t ldx, int32_t nr, int32_t n,
+                                 int32_t nout, double* __restrict__ XT) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nout * kMaxRhs) return;
+    const int32_t j = (int32_t)(t / kMaxRhs);
+    const int c = (int)(t % kMaxRhs);
+    XT[t] = (c < nr && j < n) ? X[(size_t)c * ldx + j] : 0.0;
+}
+
+// Columns [lo, hi) of chunk ch for the 128-row tile at rb0 (empty when lo >= hi).
+__host__ __device__ __forceinline__ void mrhs_t_range(int tri, int32_t n, int32_t ch, int32_t rb0,
+                                                      int32_t& lo, int32_t& hi) {
+    lo = ch * kKChunk;
+    hi = min(n, lo + kKChunk);
+    if (tri == 1) hi = min(hi, rb0 + kTRows);  // lower tiles: k < tile end
+    if (tri == 2) lo = max(lo, rb0);           // upper tiles: k >= tile start
+}
+
+// part[ch][c][row] = sum_{k in chunk ch} M[row][k] X[c][k], TRI as in mrhs_t_range.
+// MT float: two 16-column groups per pass (A loads of both issued first).
+template <int TRI, typename MT>
+__global__ void __launch_bounds__(128, 4)
+mrhs_t_kernel(const MT* __restrict__ M, int32_t ldm, int32_t n, const double* __restrict__ XT,
+              double* __restrict__ part, int32_t ldp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int32_t ch = blockIdx.x, rb0 = blockIdx.y * kTRows;
+    int32_t lo, hi;
+    mrhs_t_range(TRI, n, ch, rb0, lo, hi);
+    if (lo >= hi) return;  // the reduction skips this chunk for these rows
+    const int q = lane & 3, gq = lane >> 2;
+    constexpr int kF = 4;                       // m8 fragments per warp
+    constexpr int kG = sizeof(MT) == 4 ? 2 : 1; // 16-column groups per pass
+    const MT* mrow[kF];
+    bool rin[kF];
+#pragma unroll
+    for (int f = 0; f < kF; f++) {
+        const int32_t row = rb0 + warp * 32 + 8 * f + gq;
+        rin[f] = row < n;
+        mrow[f] = M + (size_t)(rin[f] ? row : 0) * ldm;
+    }
+    const bool vec = sizeof(MT) == 8 ? (ldm & 1) == 0 : (ldm & 3) == 0;
+    double acc[kF][4];
+#pragma unroll
+    for (int f = 0; f < kF; f++) acc[f][0] = acc[f][1] = acc[f][2] = acc[f][3] = 0.0;
+    for (int32_t g0 = lo; g0 < hi; g0 += 16 * kG) {
+        MT a[kG][kF][4];
+        double b0[kG][4], b1[kG][4];
+#pragma unroll
+        for (int u = 0; u < kG; u++) {
+            const int32_t g = g0 + 16 * u;
+            const int32_t col = g + 4 * q;
+#pragma unroll
+            for (int f = 0; f < kF; f++) {
+                if (g < hi && rin[f] && vec && col + 3 < hi) {
+                    if constexpr (sizeof(MT) == 8) {
+                        const double2 p0 = *reinterpret_cast<const double2*>(mrow[f] + col);
+                        const double2 p1 = *reinterpret_cast<const double2*>(mrow[f] + col + 2);
+                        a[u][f][0] = p0.x;
+                        a[u][f][1] = p0.y;
+                        a[u][f][2] = p1.x;
+                        a[u][f][3] = p1.y;
+                    } else {
+                        const float4 p0 = *reinterpret_cast<const float4*>(mrow[f] + col);
+                        a[u][f][0] = p0.x;
+                        a[u][f][1] = p0.y;
+                        a[u][f][2] = p0.z;
+                        a[u][f][3] = p0.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 4; t++)
+                        a[u][f][t] = (g < hi && rin[f] && col + t < hi) ? mrow[f][col + t] : (MT)0;
+                }
+            }
+            // B: slot q <-> column g + 4 q + s4; rows past n are zero in XT
+#pragma unroll
+            for (int s4 = 0; s4 < 4; s4++) {
+                const double* xr = XT + (size_t)(g < hi ? col + s4 : 0) * kMaxRhs;
+                b0[u][s4] = g < hi ? xr[gq] : 0.0;
+                b1[u][s4] = g < hi ? xr[8 + gq] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kG; u++) {
+#pragma unroll
+            for (int s4 = 0; s4 < 4; s4++) {
+#pragma unroll
+                for (int f = 0; f < kF; f++) {
+                    dmma884(acc[f][0], acc[f][1], (double)a[u][f][s4], b0[u][s4]);
+                    dmma884(acc[f][2], acc[f][3], (double)a[u][f][s4], b1[u][s4]);
+                }
+            }
+        }
+    }
+    const int cb = 2 * q;
+    double* P = part + (size_t)ch * kMaxRhs * ldp;
+#pragma unroll
+    for (int f = 0; f < kF; f++) {
+        if (!rin[f]) continue;
+        const int32_t row = rb0 + warp * 32 + 8 * f + gq;
+        P[(size_t)cb * ldp + row] = acc[f][0];
+        P[(size_t)(cb + 1) * ldp + row] = acc[f][1];
+        P[(size_t)(8 + cb) * ldp + row] = acc[f][2];
+        P[(size_t)(9 + cb) * ldp + row] = acc[f][3];
+    }
+}
+
+// Y[c][i] = scale_i (sum over the row's non-empty chunks of part[ch][c][i] +
+// shift sum_z spart[z][c]) for i < n, c < nr (scale, spart optional); also
+// YT[i][c] when YT is given (its columns c >= nr stay as they are: zero).
+__global__ void mrhs_t_reduce_kernel(const double* __restrict__ part, int32_t ldp, int tri,
+                                     int32_t n, int32_t nr, const double* __restrict__ scale,
+                                     double shift, const double* __restrict__ spart, int32_t nz,
+                                     double* __restrict__ Y, int32_t ldy, double* __restrict__ YT) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nr * n) return;
+    const int c = (int)(t / n);
+    const int32_t i = (int32_t)(t % n);
+    const int32_t rb0 = i / kTRows * kTRows;
+    const int32_t nch = (n + kKChunk - 1) / kKChunk;
+    double acc = 0.0;
+    for (int32_t ch = 0; ch < nch; ch++) {
+        int32_t lo, hi;
+        mrhs_t_range(tri, n, ch, rb0, lo, hi);
+        if (lo < hi) acc += part[((size_t)ch * kMaxRhs + c) * ldp + i];
+    }
+    if (spart) {
+        double sc = 0.0;
+        for (int32_t z = 0; z < nz; z++) sc += spart[(size_t)z * kMaxRhs + c];
+        acc += shift * sc;
+    }
+    if (scale) acc *= scale[i];
+    if (Y) Y[(size_t)c * ldy + i] = acc;
+    if (YT) YT[(size_t)i * kMaxRhs + c] = acc;
 }
 
 // Y[c][i] = scale_i (sum_z part[z][c][i] + shift s[c]) for i < n (scale, s optional).
@@ -1229,22 +1393,28 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
     *converged = true;
     *iters = 0;
     const size_t vec = (size_t)kMaxRhs * Vp;
-    TPE_TRY(ensure(ctx, ctx->mx_vec, sizeof(double) * (6 * vec + 8 * kMaxRhs + kMaxRhs * kDotChunks)));
-    constexpr int kSplit = 8;
-    TPE_TRY(ensure(ctx, ctx->mx_part, sizeof(double) * (size_t)kSplit * kMaxRhs * Vp));
+    const int32_t nz = (Vp + 255) / 256;  // 256-row blocks of the matvec's column sums
+    TPE_TRY(ensure(ctx, ctx->mx_vec, sizeof(double) * (8 * vec + 8 * kMaxRhs + kMaxRhs * kDotChunks +
+                                                       (size_t)nz * kMaxRhs)));
+    // split-K partial sums of the right-hand-side-major products: one slot per
+    // column chunk
+    const int32_t nch = (Vp + kKChunk - 1) / kKChunk;
+    TPE_TRY(ensure(ctx, ctx->mx_part, sizeof(double) * (size_t)nch * kMaxRhs * Vp));
     double* X = ctx->mx_vec.as<double>();
     double* R = X + vec;
     double* P = R + vec;
     double* Q = P + vec;
     double* Zv = Q + vec;
     double* U = Zv + vec;
-    double* sc = U + vec;  // 8 arrays of kMaxRhs scalars
-    double* s_sum = sc;
+    double* XT = U + vec;   // a product's input, right-hand-side major (Vp x 16)
+    double* UT = XT + vec;  // the preconditioner's middle vector, the same way
+    double* sc = UT + vec;  // 8 arrays of kMaxRhs scalars
     double* pq = sc + kMaxRhs;
     double* rz[2] = {sc + 2 * kMaxRhs, sc + 3 * kMaxRhs};
     double* res2 = sc + 4 * kMaxRhs;
     double* bn2 = sc + 5 * kMaxRhs;
     double* dpart = sc + 8 * kMaxRhs;  // kMaxRhs x kDotChunks partial dot products
+    double* spart = dpart + kMaxRhs * kDotChunks;  // nz x kMaxRhs column sums of the matvec
     double* part = ctx->mx_part.as<double>();
     const double* d = ctx->mx_d.as<double>();
     const float* Zf = ctx->mx_Zd.as<float>();
@@ -1254,30 +1424,34 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
     // the predicted stop below
     std::vector<double> hist((size_t)(kRateSpan + 1) * kMaxRhs);
     int32_t max_iters = 0;
-    const unsigned rb_V = (unsigned)((V + kMvRows - 1) / kMvRows);
-    const unsigned rb_Vp = (unsigned)(Vp / kMvRows);
+    const dim3 grid_p((unsigned)nch, (unsigned)(Vp / kTRows));
+    const dim3 grid_a((unsigned)((V + kKChunk - 1) / kKChunk), (unsigned)((V + kTRows - 1) / kTRows));
     for (int32_t c0 = 0; c0 < nr; c0 += kMaxRhs) {
         const int32_t n = nr - c0 < kMaxRhs ? nr - c0 : kMaxRhs;
         const int64_t tot = (int64_t)n * Vp;
+        // UT's columns n .. 15 stay zero through the pass (the reductions write
+        // columns < n only)
+        TPE_CUDA_TRY(cudaMemsetAsync(UT, 0, sizeof(double) * vec, st));
         // out = W (Z in): the preconditioner (L L^T)^{-1} of the scaled system
         auto precond = [&](const double* in, double* out) -> int32_t {
-            KernelScope ks(ctx, TPE_KGROUP_TRSV, 4);
-            mrhs_dmma_kernel<1, float><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Zf, Vp, Vp, in, Vp, n, part);
-            mrhs_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, kSplit, Vp, Vp, n, nullptr, 0.0,
-                                                                nullptr, U);
-            mrhs_dmma_kernel<2, float><<<dim3(rb_Vp, kSplit), 256, 0, st>>>(Wf, Vp, Vp, U, Vp, n, part);
-            mrhs_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, kSplit, Vp, Vp, n, nullptr, 0.0,
-                                                                nullptr, out);
+            KernelScope ks(ctx, TPE_KGROUP_TRSV, 5);
+            rhs_major_kernel<<<nblk(vec, 256), 256, 0, st>>>(in, Vp, n, Vp, Vp, XT);
+            mrhs_t_kernel<1, float><<<grid_p, 128, 0, st>>>(Zf, Vp, Vp, XT, part, Vp);
+            mrhs_t_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, Vp, 1, Vp, n, nullptr, 0.0,
+                                                                  nullptr, 0, nullptr, Vp, UT);
+            mrhs_t_kernel<2, float><<<grid_p, 128, 0, st>>>(Wf, Vp, Vp, UT, part, Vp);
+            mrhs_t_reduce_kernel<<<nblk(tot, 256), 256, 0, st>>>(part, Vp, 2, Vp, n, nullptr, 0.0,
+                                                                  nullptr, 0, out, Vp, nullptr);
             TPE_CUDA_TRY(cudaGetLastError());
             return TPE_OK;
         };
         // out = S in = D (A + shift 1 1^T) D in, rows < V
         auto matvec = [&](const double* in, double* out) -> int32_t {
             KernelScope ks(ctx, TPE_KGROUP_OTHER, 3);
-            cg_prep_kernel<<<n, 256, 0, st>>>(in, d, V, Vp, U, s_sum);
-            mrhs_dmma_kernel<0, double><<<dim3(rb_V, kSplit), 256, 0, st>>>(d_A, V, V, U, Vp, n, part);
-            mrhs_reduce_kernel<<<nblk((int64_t)n * V, 256), 256, 0, st>>>(part, kSplit, V, Vp, n, d,
-                                                                           shift, s_sum, out);
+            cg_prep_t_kernel<<<nz, 256, 0, st>>>(in, d, V, Vp, n, XT, spart);
+            mrhs_t_kernel<0, double><<<grid_a, 128, 0, st>>>(d_A, V, V, XT, part, Vp);
+            mrhs_t_reduce_kernel<<<nblk((int64_t)n * V, 256), 256, 0, st>>>(part, Vp, 0, V, n, d, shift,
+                                                                             spart, nz, out, Vp, nullptr);
             TPE_CUDA_TRY(cudaGetLastError());
             return TPE_OK;
         };

@@ -43,6 +43,29 @@ __device__ __forceinline__ double pow_b(double x, double b) {
     return pow(x, b);
 }
 
+// s = sqrt(x), inv_s = 1/s (0 below 1e-14) and inv_se = 1/(s + eps) for x >= 0,
+// from one reciprocal square root r: s = x r and 1/(s + eps) = r / (1 + t) with
+// t = eps r, summed as r (1 - t + t^2) when t < 2^-20 (the first term left out
+// is below 2^-60 relative). Distances within about 1e6 eps of zero (and
+// non-finite input) take the square root and the divisions themselves.
+__device__ __forceinline__ void dist_terms(double x, double eps, double& s, double& inv_s,
+                                           double& inv_se) {
+    const double r = rsqrt(x);
+    const double t = eps * r;
+    if (t < 9.5367431640625e-07) {
+        s = x * r;
+        inv_s = r;
+        inv_se = fma(-r, t * (1.0 - t), r);
+    } else {
+        s = sqrt(x);
+        inv_s = s < 1e-14 ? 0.0 : 1.0 / s;
+        inv_se = 1.0 / (s + eps);
+    }
+}
+
+// sqrt(x) for x >= 0 from a reciprocal square root (0 at x = 0).
+__device__ __forceinline__ double sqrt_r(double x) { return x > 0.0 ? x * rsqrt(x) : sqrt(x); }
+
 __device__ __forceinline__ bool disjoint(int2 a, int2 b) {
     return a.x != b.x && a.x != b.y && a.y != b.x && a.y != b.y;
 }
@@ -261,19 +284,20 @@ energy_sym_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb
                 const double qx = (s2 & 1) ? qb.x : qa.x, qy = (s2 & 1) ? qb.y : qa.y,
                              qz = (s2 & 1) ? qb.z : qa.z;
                 const double dx = px - qx, dy = py - qy, dz = pz - qz;
-                const double invDn = 1.0 / (sqrt(dx * dx + dy * dy + dz * dz) + eps);
+                double dn, invD, invDn;
+                dist_terms(dx * dx + dy * dy + dz * dz, eps, dn, invD, invDn);
                 const double iDb = (MODE == 1) ? pow_b<1>(invDn, beta) : 0.0;
                 const double cx = eIy * dz - eIz * dy, cy = eIz * dx - eIx * dz,
                              cz = eIx * dy - eIy * dx;
-                const double cn = sqrt(cx * cx + cy * cy + cz * cz) + eps;
+                const double cn = sqrt_r(cx * cx + cy * cy + cz * cz) + eps;
                 const double kx = eJy * dz - eJz * dy, ky = eJz * dx - eJx * dz,
                              kz = eJx * dy - eJy * dx;
-                const double kn = sqrt(kx * kx + ky * ky + kz * kz) + eps;
+                const double kn = sqrt_r(kx * kx + ky * ky + kz * kz) + eps;
                 if (MODE == 1) {
                     sumF += pow_a<1>(cn, alpha) * iDb;
                     sumF2 += pow_a<1>(kn, alpha) * iDb;
                 } else {
-                    const double den = pow(1.0 / invDn, beta);
+                    const double den = pow(dn + eps, beta);
                     sumF += pow(cn, alpha) / den;
                     sumF2 += pow(kn, alpha) / den;
                 }
@@ -301,14 +325,20 @@ __device__ __forceinline__ double kd_vec(double ex, double ey, double ez, double
     const double cx = ey * dz - ez * dy;
     const double cy = ez * dx - ex * dz;
     const double cz = ex * dy - ey * dx;
-    const double rc = sqrt(cx * cx + cy * cy + cz * cz);
+    const double c2 = cx * cx + cy * cy + cz * cz;
+    double rc, inv = 0.0;
+    if (c2 >= 1e-28) {
+        inv = rsqrt(c2);
+        rc = c2 * inv;
+    } else {
+        rc = sqrt(c2);
+    }
     const double ce = rc + eps;
     const double f = pow_a<MODE>(ce, alpha) * invDPowB;
     const double coeff_c = alpha * pow_a1<MODE>(ce, alpha) * invDPowB;
     const double coeff_d = -beta * f * invDe;
     double ux = 0, uy = 0, uz = 0, vx = 0, vy = 0, vz = 0;
-    if (rc >= 1e-14) {
-        const double inv = 1.0 / rc;
+    if (c2 >= 1e-28) {
         ux = inv * (cy * ez - cz * ey);
         uy = inv * (cz * ex - cx * ez);
         uz = inv * (cx * ey - cy * ex);
@@ -434,15 +464,9 @@ __device__ __forceinline__ void grad_sym_tile(int x, int tid, int bar, GradSmem&
                 const double px = ai ? b.x : a.x, py = ai ? b.y : a.y, pz = ai ? b.z : a.z;
                 const double qx = bk ? qb.x : qa.x, qy = bk ? qb.y : qa.y, qz = bk ? qb.z : qa.z;
                 const double dx = px - qx, dy = py - qy, dz = pz - qz;  // p_I - p_J
-                const double rd = sqrt(dx * dx + dy * dy + dz * dz);
-                double hx = 0, hy = 0, hz = 0;
-                if (!(rd < 1e-14)) {
-                    const double inv = 1.0 / rd;
-                    hx = inv * dx;
-                    hy = inv * dy;
-                    hz = inv * dz;
-                }
-                const double invDe = 1.0 / (rd + eps);
+                double rd, inv, invDe;
+                dist_terms(dx * dx + dy * dy + dz * dz, eps, rd, inv, invDe);
+                const double hx = inv * dx, hy = inv * dy, hz = inv * dz;
                 const double invDPowB = (MODE == 1) ? pow_b<1>(invDe, beta) : 1.0 / pow(rd + eps, beta);
                 double ddIJ[3], deIJ[3], ddJI[3], deJI[3];
                 sumF += kd_vec<MODE>(eIx, eIy, eIz, dx, dy, dz, hx, hy, hz, invDPowB, invDe, alpha,
