@@ -1321,6 +1321,9 @@ int32_t tpe_set_topology(tpe_ctx* ctx, const int32_t* edges, int32_t E, int32_t 
         ctx->V = V;
         ctx->E = E;
         ctx->h_edges.assign(edges, edges + 2 * (size_t)E);
+        ctx->closed_loop = E == V && V >= 8;
+        for (int32_t I = 0; I < E && ctx->closed_loop; I++)
+            ctx->closed_loop = edges[2 * I] == I && edges[2 * I + 1] == (I + 1 == V ? 0 : I + 1);
         ctx->h_inc_off.assign((size_t)V + 1, 0);
         for (int32_t I = 0; I < E; I++) {
             ctx->h_inc_off[edges[2 * I] + 1]++;

@@ -302,6 +302,159 @@ gather_A_kernel(const double2* __restrict__ M, int32_t E, const int32_t* __restr
     }
 }
 
+// ---- closed single loop: A straight from the pair weights -------------------
+//
+// When the curve is one closed loop with edge I = (I, I+1 mod V) (E = V), vertex
+// v is the second vertex of edge v-1 and the first of edge v, so
+//   A[v][u] = sum_{I in {v-1, v}} sum_{J in {u-1, u}} s_vI s_uJ Mb'[I][J] + M0'[I][J]
+// (s = +1 for the first vertex, -1 for the second): a 2 x 2 stencil on the pair
+// matrix. One block per lower-triangular 32 x 32 vertex tile computes the
+// 33 x 33 pair weights of its edges and the one edge before (shared memory) and
+// writes A's tile and its mirror once each; nothing of size E^2 is stored. The
+// pair matrix's diagonal (the row sums) is added to A's cyclic band afterwards
+// (loop_band_kernel), from the same per-tile row sums as the general path.
+constexpr int kLT = 32;       // vertex tile
+constexpr int kLH = kLT + 1;  // edges per side: the tile's own and the one before
+
+template <int MODE>
+__global__ void __launch_bounds__(256)
+assemble_loop_kernel(const double4* __restrict__ ea, const double4* __restrict__ eb,
+                     const int2* __restrict__ edges, int32_t V, double distExp, double eps,
+                     double* __restrict__ A, double2* __restrict__ rowpart) {
+    __shared__ EdgeRec sI[kLH], sJ[kLH];
+    __shared__ double2 W[kLH][kLH + 1];  // (Mb', M0') of edge pair (k, l)
+    // the symmetric weights w of the same pairs, then (after the row sums) the
+    // A tile staged for its mirror
+    __shared__ double2 wr_raw[kLH * (kLH + 1)];
+    double2(*Wr)[kLH + 1] = reinterpret_cast<double2(*)[kLH + 1]>(wr_raw);
+    double(*ta)[kLT + 1] = reinterpret_cast<double(*)[kLT + 1]>(wr_raw);
+    static_assert(sizeof(double) * kLT * (kLT + 1) <= sizeof(double2) * kLH * (kLH + 1),
+                  "the staged A tile fits in the weights' space");
+    const int32_t t = blockIdx.x;
+    int32_t ti = (int32_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((int64_t)ti * (ti + 1) / 2 > t) ti--;
+    while ((int64_t)(ti + 1) * (ti + 2) / 2 <= t) ti++;
+    const int32_t tj = t - ti * (ti + 1) / 2;
+    const int32_t v0 = ti * kLT, u0 = tj * kLT;
+    const int tid = threadIdx.x;
+    // edge index of row k: k = 0 is the edge before the tile, k >= 1 edge v0 + k - 1
+    auto edge_of = [&](int32_t w0, int k) -> int32_t {
+        if (k == 0) return w0 == 0 ? V - 1 : w0 - 1;
+        const int32_t I = w0 + k - 1;
+        return I < V ? I : -1;
+    };
+    if (tid < kLH) {
+        const int32_t I = edge_of(v0, tid);
+        load_edge(ea, eb, edges, V, I < 0 ? V : I, sI[tid]);  // I = V: an empty record
+    } else if (tid < 2 * kLH) {
+        const int32_t J = edge_of(u0, tid - kLH);
+        load_edge(ea, eb, edges, V, J < 0 ? V : J, sJ[tid - kLH]);
+    }
+    __syncthreads();
+    for (int e = tid; e < kLH * kLH; e += blockDim.x) {
+        const int k = e / kLH, l = e % kLH;
+        const EdgeRec& a = sI[k];
+        const EdgeRec& b = sJ[l];
+        const int32_t I = edge_of(v0, k), J = edge_of(u0, l);
+        double2 out = make_double2(0.0, 0.0), w = out;
+        const bool ok = I >= 0 && J >= 0 && I != J && a.ij.x != b.ij.x && a.ij.x != b.ij.y &&
+                        a.ij.y != b.ij.x && a.ij.y != b.ij.y;
+        if (ok) {
+            w = pair_weight<MODE>(a, b, distExp, eps);
+            const double dotT = a.T.x * b.T.x + a.T.y * b.T.y + a.T.z * b.T.z;
+            out = make_double2(-w.x * dotT / (a.p1.w * b.p1.w), -w.y);
+        }
+        W[k][l] = out;
+        Wr[k][l] = w;
+    }
+    __syncthreads();
+    // row sums of the tile's own edges (k, l >= 1): row I over tile tj's edges,
+    // and (off-diagonal tiles) row J over tile ti's edges
+    if (tid < kLT) {
+        const int32_t I = v0 + tid;
+        if (I < V) {
+            double2 rs = make_double2(0.0, 0.0);
+            for (int l = 1; l < kLH; l++) {
+                rs.x += Wr[tid + 1][l].x;
+                rs.y += Wr[tid + 1][l].y;
+            }
+            rowpart[(int64_t)tj * V + I] = rs;
+        }
+    } else if (tid < 2 * kLT && ti != tj) {
+        const int c = tid - kLT;
+        const int32_t J = u0 + c;
+        if (J < V) {
+            double2 cs = make_double2(0.0, 0.0);
+            for (int k = 1; k < kLH; k++) {
+                cs.x += Wr[k][c + 1].x;
+                cs.y += Wr[k][c + 1].y;
+            }
+            rowpart[(int64_t)ti * V + J] = cs;
+        }
+    }
+    __syncthreads();  // the row sums have read Wr; ta takes its place
+    // A[v][u] for the tile (rows v0 + r, columns u0 + c, u <= v), the incident
+    // edges of each vertex in ascending edge order
+    for (int e = tid; e < kLT * kLT; e += blockDim.x) {
+        const int r = e / kLT, c = e % kLT;
+        const int32_t v = v0 + r, u = u0 + c;
+        double sb = 0.0, s0 = 0.0;
+        if (v < V && u < V && u <= v) {
+            // (row index in W, sign): v's edges v-1 (second vertex, -1) and v (+1)
+            int kp[2], lq[2];
+            double sp[2], sq[2];
+            if (v == 0) { kp[0] = 1; sp[0] = 1.0; kp[1] = 0; sp[1] = -1.0; }
+            else { kp[0] = r; sp[0] = -1.0; kp[1] = r + 1; sp[1] = 1.0; }
+            if (u == 0) { lq[0] = 1; sq[0] = 1.0; lq[1] = 0; sq[1] = -1.0; }
+            else { lq[0] = c; sq[0] = -1.0; lq[1] = c + 1; sq[1] = 1.0; }
+#pragma unroll
+            for (int p = 0; p < 2; p++)
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const double2 m = W[kp[p]][lq[q]];
+                    sb += sp[p] * sq[q] * m.x;
+                    s0 += m.y;
+                }
+        }
+        ta[r][c] = sb + s0;
+    }
+    __syncthreads();
+    for (int e = tid; e < kLT * kLT; e += blockDim.x) {
+        const int r = e / kLT, c = e % kLT;
+        const int32_t v = v0 + r, u = u0 + c;
+        if (v < V && u < V && u <= v) A[(int64_t)v * V + u] = ta[r][c];
+        // mirror: entry (u0 + r, v0 + c) = value (v0 + c, u0 + r)
+        const int32_t mr = u0 + r, mc = v0 + c;
+        if (mc < V && mr < V && mr < mc) A[(int64_t)mr * V + mc] = ta[c][r];
+    }
+}
+
+// The pair matrix's diagonal on A's cyclic band: for each vertex v, the terms
+// with I = J of the stencil: A[v][v] += Mb'_{v-1} + Mb'_v + M0'_{v-1} + M0'_v,
+// A[v][v+1] = A[v+1][v] += -Mb'_v + M0'_v, with (Mb'_I, M0'_I) = (d_I / l_I^2, d0_I)
+// summed from the per-tile row sums in tile order (as pair_diag_kernel).
+__global__ void loop_band_kernel(const double4* __restrict__ ea, int32_t V, int32_t nt,
+                                 const double2* __restrict__ rowpart, double* __restrict__ A) {
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    auto diag = [&](int32_t I) -> double2 {
+        double sx = 0.0, sy = 0.0;
+        for (int32_t s = 0; s < nt; s++) {
+            const double2 p = rowpart[(int64_t)s * V + I];
+            sx += p.x;
+            sy += p.y;
+        }
+        const double ell = ea[I].w;
+        return make_double2(sx / (ell * ell), sy);
+    };
+    const double2 dv = diag(v), dp = diag(v == 0 ? V - 1 : v - 1);
+    A[(int64_t)v * V + v] += (dp.x + dv.x) + (dp.y + dv.y);
+    const int32_t u = v + 1 == V ? 0 : v + 1;
+    const double off = -dv.x + dv.y;
+    A[(int64_t)v * V + u] += off;
+    A[(int64_t)u * V + v] += off;
+}
+
 }  // namespace
 
 int32_t gather_A_launch(tpe_ctx* ctx, double* d_A, double* d_B, double* d_B0) {
@@ -319,6 +472,32 @@ int32_t gather_A_launch(tpe_ctx* ctx, double* d_A, double* d_B, double* d_B0) {
 int32_t assemble_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_A,
                       double* d_B, double* d_B0) {
     const int32_t E = ctx->E;
+    if (ctx->closed_loop && !d_B && !d_B0) {
+        // one closed loop: A straight from the pair weights (no E x E matrix)
+        const int32_t V = ctx->V;
+        const double s = (beta - 1.0) / alpha;
+        const double distExp = 2.0 * (s - 1.0) + 1.0;
+        const int32_t nt = (V + kLT - 1) / kLT;
+        const int64_t tiles = (int64_t)nt * (nt + 1) / 2;
+        TPE_TRY(ensure(ctx, ctx->tmp, sizeof(double2) * (size_t)nt * V));
+        {
+            KernelScope ks(ctx, TPE_KGROUP_PAIR_WEIGHTS, 1);
+            if (alpha == 3.0 && beta == 6.0)
+                assemble_loop_kernel<1><<<(unsigned)tiles, 256, 0, ctx->stream>>>(
+                    ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), V,
+                    distExp, eps, d_A, ctx->tmp.as<double2>());
+            else
+                assemble_loop_kernel<0><<<(unsigned)tiles, 256, 0, ctx->stream>>>(
+                    ctx->edge_a.as<double4>(), ctx->edge_b.as<double4>(), ctx->d_edges.as<int2>(), V,
+                    distExp, eps, d_A, ctx->tmp.as<double2>());
+            TPE_CUDA_TRY(cudaGetLastError());
+        }
+        KernelScope ks(ctx, TPE_KGROUP_GATHER_A, 1);
+        loop_band_kernel<<<(V + 255) / 256, 256, 0, ctx->stream>>>(ctx->edge_a.as<double4>(), V, nt,
+                                                                 ctx->tmp.as<double2>(), d_A);
+        TPE_CUDA_TRY(cudaGetLastError());
+        return TPE_OK;
+    }
     TPE_TRY(ensure(ctx, ctx->pairM, sizeof(double2) * (size_t)E * E));
     const double s = (beta - 1.0) / alpha;
     const double sigma = s - 1.0;

@@ -131,6 +131,9 @@ struct tpe_ctx {
     // topology
     bool has_topology = false;
     int32_t V = 0, E = 0;
+    // one closed loop with edge I = (I, I+1 mod V), V >= 8: Gram assembly by the
+    // fused stencil kernel (assembly.cu)
+    bool closed_loop = false;
     std::vector<int32_t> h_edges;     // 2E
     std::vector<int32_t> h_inc_off;   // V+1
     std::vector<int32_t> h_inc;       // 2E entries: edge*2 + slot, ascending edge order per vertex

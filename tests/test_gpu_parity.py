@@ -285,3 +285,20 @@ def test_raw_gradient_step(mode):
     en = O.energy(r["vertices"], e)
     assert abs(r["energy"] - en) <= 1e-10 * abs(en)
     assert "field" not in T.step(v, e, None, {"mode": mode, "stepSize": s})
+
+
+@pytest.mark.parametrize("V", [8, 33, 301, 1000])
+def test_closed_loop_assembly_vs_oracle(V):
+    """A of a single closed loop (edge I = (I, I+1 mod V)) comes from the fused
+    stencil kernel; the same loop with its edges listed in another order takes
+    the general pair-matrix path. Both against the oracle's assembleAFlat."""
+    v, e = F.random_walk_knot(V, seed=60 + V)
+    want = O.assemble(v, e, "A")
+    A = T.assembleAFlat(v, e)
+    assert relerr(A, want) <= 1e-12
+    assert np.array_equal(A, A.T)
+    perm = np.roll(np.arange(V), 3)
+    e2 = np.ascontiguousarray(e[perm])
+    A2 = T.assembleAFlat(v, e2)
+    assert relerr(A2, O.assemble(v, e2, "A")) <= 1e-12
+    assert relerr(A, A2) <= 1e-12
