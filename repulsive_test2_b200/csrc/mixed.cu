@@ -118,10 +118,9 @@ constexpr int kOffTsc = kOffP + kPSize;               // 2 x 32 x kTs3
 constexpr int kOffRd = kOffTsc + 2 * 32 * kTs3;       // 128
 constexpr int kOffZdT = kOffRd + kT;                  // 32 x kS3: Z_dd^T of the current panel
 constexpr int kOffLt = kOffZdT + 32 * kS3;            // 32 x kS3: L_dd^T (wf32 scratch)
-constexpr int kOffC4 = kOffLt + 32 * kS3;             // 32 float4 (wf32 scratch)
-constexpr int kSmem3Floats = kOffC4 + 128;
+constexpr int kSmem3Floats = kOffLt + 32 * kS3;
 static_assert(kOffZ % 4 == 0 && kOffP % 4 == 0 && kOffTsc % 4 == 0 && kOffZdT % 4 == 0 &&
-              kOffLt % 4 == 0 && kOffC4 % 4 == 0, "float4 alignment");
+              kOffLt % 4 == 0, "float4 alignment");
 
 __device__ __forceinline__ void tri_decode(int e, int& ti, int& tj) {
     int t = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
@@ -138,18 +137,15 @@ __device__ __forceinline__ float f4(const float4& v, int i) {
 }
 
 // One warp factors the 32 x 32 diagonal part at (c0, c0) of a (lane = row) and
-// inverts it. Columns in groups of four: inside a group the rank-1 updates use
-// shuffles; the group's four columns then go to shared memory once (one
-// float4 per row) and the later columns take a rank-4 update from 16-byte
-// loads. The inverse (lane = column of Z) reads L column-wise from a
-// transposed copy. Writes L to a, Z (lower) to z, Z^T to zdt, 1/L_ii to rd.
+// inverts it: one rank-1 update per column by shuffles, with each column's
+// pivot formed ahead on its own lane. The inverse (lane = column of Z) reads L
+// column-wise from a transposed copy. Writes L to a, Z (lower) to z, Z^T to zdt, 1/L_ii to rd.
 __device__ __noinline__ void warp_factor32(float* sm, int c0, int lane, int32_t* bad) {
     float* a = sm + kOffA;
     float* z = sm + kOffZ;
     float* rd = sm + kOffRd;
     float* zdt = sm + kOffZdT;
     float* lt = sm + kOffLt;
-    float4* c4 = reinterpret_cast<float4*>(sm + kOffC4);
     float v[32];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -161,43 +157,30 @@ __device__ __noinline__ void warp_factor32(float* sm, int c0, int lane, int32_t*
     }
     bool brk = false;
     float myrs = 1.0f;
+    // The pivot of column K + 1 is formed on its own lane right after column K
+    // (dn = v[K+1] - L[K+1][K]^2: the last update of that diagonal entry uses
+    // the lane's own value) and broadcast before column K's other updates, so
+    // the pivot chain holds one shuffle per column; the updates themselves run
+    // in the same order as one rank-1 update per column.
+    float piv = __shfl_sync(0xffffffffu, v[0], 0);
 #pragma unroll
-    for (int g = 0; g < 8; g++) {
-#pragma unroll
-        for (int kk = 0; kk < 4; kk++) {
-            const int K = 4 * g + kk;
-            float piv = __shfl_sync(0xffffffffu, v[K], K);
-            if (!(piv > 0.0f) || !isfinite(piv)) {
-                brk = true;
-                piv = 1.0f;
-            }
-            const float rs = rsqrtf(piv);
-            const float lk = (lane == K) ? piv * rs : v[K] * rs;
-            if (lane >= K) v[K] = lk;
-            if (lane == K) myrs = rs;
-#pragma unroll
-            for (int m = K + 1; m < 4 * g + 4; m++) {
-                const float lmk = __shfl_sync(0xffffffffu, lk, m);
-                if (lane >= m) v[m] = fmaf(-lk, lmk, v[m]);
-            }
+    for (int K = 0; K < 32; K++) {
+        if (!(piv > 0.0f) || !isfinite(piv)) {
+            brk = true;
+            piv = 1.0f;
         }
-        if (g < 7) {
-            c4[lane] = make_float4(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
-            __syncwarp();
+        const float rs = rsqrtf(piv);
+        const float lk = (lane == K) ? piv * rs : v[K] * rs;  // L[lane][K] (lanes >= K)
+        if (lane >= K) v[K] = lk;
+        if (lane == K) myrs = rs;
+        float pnext = 0.0f;
+        if (K + 1 < 32) pnext = __shfl_sync(0xffffffffu, fmaf(-lk, lk, v[K + 1]), K + 1);
 #pragma unroll
-            for (int m = 4 * g + 4; m < 32; m++) {
-                const float4 q = c4[m];
-                if (lane >= m) {
-                    float t = v[m];
-                    t = fmaf(-v[4 * g], q.x, t);
-                    t = fmaf(-v[4 * g + 1], q.y, t);
-                    t = fmaf(-v[4 * g + 2], q.z, t);
-                    t = fmaf(-v[4 * g + 3], q.w, t);
-                    v[m] = t;
-                }
-            }
-            __syncwarp();
+        for (int m = K + 1; m < 32; m++) {
+            const float lmk = __shfl_sync(0xffffffffu, lk, m);
+            if (lane >= m) v[m] = fmaf(-lk, lmk, v[m]);
         }
+        piv = pnext;
     }
     if (brk && lane == 0) atomicExch(bad, 1);
     // L back to a (rows, 16-byte stores), L^T to lt (lt[k][lane] = L[lane][k]), 1/L_ii
