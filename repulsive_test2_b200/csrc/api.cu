@@ -1276,7 +1276,7 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
                       &ctx->flat3, &ctx->dir, &ctx->pairM, &ctx->edge_m, &ctx->mat_A, &ctx->mat_L,
                       &ctx->mat_Linv, &ctx->mat_B, &ctx->mat_B0, &ctx->con_C, &ctx->con_Y,
-                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->rhs,
+                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->con_part, &ctx->rhs,
                       &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status,
                       &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
                       &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,

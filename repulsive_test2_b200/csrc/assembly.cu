@@ -432,13 +432,17 @@ assemble_loop_kernel(const double4* __restrict__ ea, const double4* __restrict__
 // The pair matrix's diagonal on A's cyclic band: for each vertex v, the terms
 // with I = J of the stencil: A[v][v] += Mb'_{v-1} + Mb'_v + M0'_{v-1} + M0'_v,
 // A[v][v+1] = A[v+1][v] += -Mb'_v + M0'_v, with (Mb'_I, M0'_I) = (d_I / l_I^2, d0_I)
-// summed from the per-tile row sums in tile order (as pair_diag_kernel).
-__global__ void loop_band_kernel(const double4* __restrict__ ea, int32_t V, int32_t nt,
-                                 const double2* __restrict__ rowpart, double* __restrict__ A) {
-    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
+// summed from the per-tile row sums in tile order. Each block forms the
+// diagonal entries of its 256 vertices and of the vertex before them once, in
+// shared memory.
+__global__ void __launch_bounds__(256) loop_band_kernel(const double4* __restrict__ ea, int32_t V,
+                                                        int32_t nt, const double2* __restrict__ rowpart,
+                                                        double* __restrict__ A) {
+    __shared__ double2 dg[257];
+    const int32_t b0 = blockIdx.x * 256;
     auto diag = [&](int32_t I) -> double2 {
         double sx = 0.0, sy = 0.0;
+#pragma unroll 8
         for (int32_t s = 0; s < nt; s++) {
             const double2 p = rowpart[(int64_t)s * V + I];
             sx += p.x;
@@ -447,7 +451,12 @@ __global__ void loop_band_kernel(const double4* __restrict__ ea, int32_t V, int3
         const double ell = ea[I].w;
         return make_double2(sx / (ell * ell), sy);
     };
-    const double2 dv = diag(v), dp = diag(v == 0 ? V - 1 : v - 1);
+    const int32_t v = b0 + threadIdx.x;
+    if (v < V) dg[threadIdx.x + 1] = diag(v);
+    if (threadIdx.x == 0) dg[0] = diag(b0 == 0 ? V - 1 : b0 - 1);
+    __syncthreads();
+    if (v >= V) return;
+    const double2 dv = dg[threadIdx.x + 1], dp = dg[threadIdx.x];
     A[(int64_t)v * V + v] += (dp.x + dv.x) + (dp.y + dv.y);
     const int32_t u = v + 1 == V ? 0 : v + 1;
     const double off = -dv.x + dv.y;

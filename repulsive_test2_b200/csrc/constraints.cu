@@ -66,21 +66,31 @@ __device__ void block_reduce(double (&v)[N], bool is_max_last) {
     __syncthreads();
 }
 
-// One CTA per block: phi rows, and ns[2b] = ||phi_b||^2, ns[2b+1] = scale_b.
+// The constraint rows phi and, per block b, ns[2b] = ||phi_b||^2 and
+// ns[2b+1] = scale_b, for position set y (idx[y], or y). kPhiSplit CTAs per
+// (block, position set): CTA s takes the edges (or vertices)
+// [s E / S, (s+1) E / S) and leaves its reductions in
+// part[((y * nblocks + b) * S + s) * 5 + q]; edge-length rows are written
+// directly. phi_final_kernel then combines the S partials in order (sums in
+// order, the maxima by Math.max) and writes the block rows, norms and scales.
+constexpr int kPhiSplit = 16;
+
 __global__ void __launch_bounds__(kBS)
-phi_kernel(const double* __restrict__ pos, const int2* __restrict__ edges, int32_t E, int32_t V,
-           const DevBlock* __restrict__ blocks, double* __restrict__ phi, double* __restrict__ ns,
-           int64_t pos_stride, const int32_t* __restrict__ idx, int32_t k) {
+phi_part_kernel(const double* __restrict__ pos, const int2* __restrict__ edges, int32_t E,
+                int32_t V, const DevBlock* __restrict__ blocks, double* __restrict__ phi,
+                int64_t pos_stride, const int32_t* __restrict__ idx, int32_t k,
+                double* __restrict__ part) {
     const DevBlock B = blocks[blockIdx.x];
-    // batched form: position set idx[y] (or y), outputs of row y
-    if (gridDim.y > 1 || idx) {
-        pos += (idx ? idx[blockIdx.y] : (int32_t)blockIdx.y) * pos_stride;
-        phi += (size_t)blockIdx.y * k;
-        ns += (size_t)blockIdx.y * 2 * gridDim.x;
-    }
+    const int32_t y = blockIdx.y, sp = blockIdx.z;
+    pos += (idx ? idx[y] : y) * pos_stride;
+    phi += (size_t)y * k;
+    double* out = part + ((size_t)(y * gridDim.x + blockIdx.x) * kPhiSplit + sp) * 5;
+    const int32_t n = B.kind == TPE_BLOCK_POINT ? V : E;
+    const int32_t lo = (int32_t)((int64_t)n * sp / kPhiSplit);
+    const int32_t hi = (int32_t)((int64_t)n * (sp + 1) / kPhiSplit);
     if (B.kind == TPE_BLOCK_BARYCENTER) {
-        double v[5] = {0, 0, 0, 0, 0};  // phi x,y,z, L, R(max)
-        for (int32_t I = threadIdx.x; I < E; I += kBS) {
+        double v[5] = {0, 0, 0, 0, 0};
+        for (int32_t I = lo + threadIdx.x; I < hi; I += kBS) {
             const int2 e = edges[I];
             EdgeGeo g;
             edge_geo(pos, e, g, B.target);
@@ -96,14 +106,11 @@ phi_kernel(const double* __restrict__ pos, const int2* __restrict__ edges, int32
             v[4] = js_max(js_max(v[4], sqrt(d1)), sqrt(d2));
         }
         block_reduce<5>(v, true);
-        if (threadIdx.x == 0) {
-            for (int r = 0; r < 3; r++) phi[B.row0 + r] = v[r];
-            ns[2 * blockIdx.x] = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-            ns[2 * blockIdx.x + 1] = js_max(1.0, v[3] * js_max(1.0, v[4]));
-        }
+        if (threadIdx.x == 0)
+            for (int q = 0; q < 5; q++) out[q] = v[q];
     } else if (B.kind == TPE_BLOCK_TOTAL_LENGTH || B.kind == TPE_BLOCK_EDGE_LENGTHS) {
-        double v[2] = {0, 0};  // L, sum phi^2 (edge rows)
-        for (int32_t I = threadIdx.x; I < E; I += kBS) {
+        double v[2] = {0, 0};
+        for (int32_t I = lo + threadIdx.x; I < hi; I += kBS) {
             const int2 e = edges[I];
             EdgeGeo g;
             edge_geo(pos, e, g, nullptr);
@@ -116,18 +123,12 @@ phi_kernel(const double* __restrict__ pos, const int2* __restrict__ edges, int32
         }
         block_reduce<2>(v, false);
         if (threadIdx.x == 0) {
-            if (B.kind == TPE_BLOCK_TOTAL_LENGTH) {
-                const double p = B.L0 - v[0];
-                phi[B.row0] = p;
-                ns[2 * blockIdx.x] = p * p;
-            } else {
-                ns[2 * blockIdx.x] = v[1];
-            }
-            ns[2 * blockIdx.x + 1] = js_max(1.0, v[0]);
+            out[0] = v[0];
+            out[1] = v[1];
         }
     } else if (B.kind == TPE_BLOCK_POINT) {
-        double v[1] = {0};  // R(max)
-        for (int32_t i = threadIdx.x; i < V; i += kBS) {
+        double v[1] = {0};
+        for (int32_t i = lo + threadIdx.x; i < hi; i += kBS) {
             double d = 0;
             for (int r = 0; r < 3; r++) {
                 const double a = pos[3 * i + r] - B.target[r];
@@ -136,18 +137,59 @@ phi_kernel(const double* __restrict__ pos, const int2* __restrict__ edges, int32
             v[0] = js_max(v[0], sqrt(d));
         }
         block_reduce<1>(v, true);
-        if (threadIdx.x == 0) {
-            double s2 = 0.0;
-            for (int r = 0; r < 3; r++) {
-                const double p = (B.vertex >= 0 && B.vertex < V)
-                                     ? pos[3 * B.vertex + r] - B.target[r]
-                                     : NAN;
-                phi[B.row0 + r] = p;
-                s2 += p * p;
-            }
-            ns[2 * blockIdx.x] = s2;
-            ns[2 * blockIdx.x + 1] = js_max(1.0, v[0]);
+        if (threadIdx.x == 0) out[0] = v[0];
+    }
+}
+
+// One thread per (block, position set): the partials of phi_part_kernel in
+// order, then the block's rows, squared norm and scale.
+__global__ void phi_final_kernel(const double* __restrict__ pos, int32_t V,
+                                 const DevBlock* __restrict__ blocks, int32_t nblocks,
+                                 double* __restrict__ phi, double* __restrict__ ns,
+                                 int64_t pos_stride, const int32_t* __restrict__ idx, int32_t k,
+                                 int32_t n, const double* __restrict__ part) {
+    const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * nblocks) return;
+    const int32_t y = t / nblocks, b = t % nblocks;
+    const DevBlock B = blocks[b];
+    pos += (idx ? idx[y] : y) * pos_stride;
+    phi += (size_t)y * k;
+    ns += (size_t)y * 2 * nblocks;
+    const double* in = part + (size_t)(y * nblocks + b) * kPhiSplit * 5;
+    if (B.kind == TPE_BLOCK_BARYCENTER) {
+        double v[5] = {in[0], in[1], in[2], in[3], in[4]};
+        for (int sp = 1; sp < kPhiSplit; sp++) {
+            for (int q = 0; q < 4; q++) v[q] += in[sp * 5 + q];
+            v[4] = js_max(v[4], in[sp * 5 + 4]);
         }
+        for (int r = 0; r < 3; r++) phi[B.row0 + r] = v[r];
+        ns[2 * b] = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        ns[2 * b + 1] = js_max(1.0, v[3] * js_max(1.0, v[4]));
+    } else if (B.kind == TPE_BLOCK_TOTAL_LENGTH || B.kind == TPE_BLOCK_EDGE_LENGTHS) {
+        double v[2] = {in[0], in[1]};
+        for (int sp = 1; sp < kPhiSplit; sp++) {
+            v[0] += in[sp * 5];
+            v[1] += in[sp * 5 + 1];
+        }
+        if (B.kind == TPE_BLOCK_TOTAL_LENGTH) {
+            const double p = B.L0 - v[0];
+            phi[B.row0] = p;
+            ns[2 * b] = p * p;
+        } else {
+            ns[2 * b] = v[1];
+        }
+        ns[2 * b + 1] = js_max(1.0, v[0]);
+    } else if (B.kind == TPE_BLOCK_POINT) {
+        double v = in[0];
+        for (int sp = 1; sp < kPhiSplit; sp++) v = js_max(v, in[sp * 5]);
+        double s2 = 0.0;
+        for (int r = 0; r < 3; r++) {
+            const double p = (B.vertex >= 0 && B.vertex < V) ? pos[3 * B.vertex + r] - B.target[r] : NAN;
+            phi[B.row0 + r] = p;
+            s2 += p * p;
+        }
+        ns[2 * b] = s2;
+        ns[2 * b + 1] = js_max(1.0, v);
     }
 }
 
@@ -360,10 +402,14 @@ int32_t eval_constraints_batch(tpe_ctx* ctx, const double* d_pos, int64_t stride
                                const int32_t* d_idx, int32_t n, int32_t nblocks, int32_t k,
                                double* d_phi, double* d_ns) {
     if (nblocks == 0 || n == 0) return TPE_OK;
-    KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-    phi_kernel<<<dim3((unsigned)nblocks, (unsigned)n), kBS, 0, ctx->stream>>>(
+    TPE_TRY(ensure(ctx, ctx->con_part, sizeof(double) * (size_t)n * nblocks * kPhiSplit * 5));
+    KernelScope ks(ctx, TPE_KGROUP_OTHER, 2);
+    phi_part_kernel<<<dim3((unsigned)nblocks, (unsigned)n, kPhiSplit), kBS, 0, ctx->stream>>>(
         d_pos, ctx->d_edges.as<int2>(), ctx->E, ctx->V, ctx->con_blocks.as<DevBlock>(), d_phi,
-        d_ns, stride, d_idx, k);
+        stride, d_idx, k, ctx->con_part.as<double>());
+    phi_final_kernel<<<(unsigned)((n * nblocks + 127) / 128), 128, 0, ctx->stream>>>(
+        d_pos, ctx->V, ctx->con_blocks.as<DevBlock>(), nblocks, d_phi, d_ns, stride, d_idx, k, n,
+        ctx->con_part.as<double>());
     TPE_CUDA_TRY(cudaGetLastError());
     return TPE_OK;
 }
@@ -377,10 +423,14 @@ int32_t eval_constraints(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int
     TPE_TRY(ensure(ctx, ctx->con_phi, sizeof(double) * (size_t)(k + 2 * nblocks + 1)));
     double* dphi = ctx->con_phi.as<double>();
     double* dns = dphi + k;
-    { KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
-    phi_kernel<<<nblocks, kBS, 0, ctx->stream>>>(d_pos, ctx->d_edges.as<int2>(), E, V,
-                                                 ctx->con_blocks.as<DevBlock>(), dphi, dns, 0,
-                                                 nullptr, k); }
+    TPE_TRY(ensure(ctx, ctx->con_part, sizeof(double) * (size_t)nblocks * kPhiSplit * 5));
+    { KernelScope ks(ctx, TPE_KGROUP_OTHER, 2);
+    phi_part_kernel<<<dim3((unsigned)nblocks, 1, kPhiSplit), kBS, 0, ctx->stream>>>(
+        d_pos, ctx->d_edges.as<int2>(), E, V, ctx->con_blocks.as<DevBlock>(), dphi, 0, nullptr, k,
+        ctx->con_part.as<double>());
+    phi_final_kernel<<<(unsigned)((nblocks + 127) / 128), 128, 0, ctx->stream>>>(
+        d_pos, V, ctx->con_blocks.as<DevBlock>(), nblocks, dphi, dns, 0, nullptr, k, 1,
+        ctx->con_part.as<double>()); }
     TPE_CUDA_TRY(cudaGetLastError());
     if (d_C) {
         TPE_CUDA_TRY(cudaMemsetAsync(d_C, 0, sizeof(double) * (size_t)k * 3 * V, ctx->stream));

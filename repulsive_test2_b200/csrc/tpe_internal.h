@@ -152,6 +152,7 @@ struct tpe_ctx {
     tpe::DevBuf edge_m;                     // mixed-precision edge records (4 float4 per edge)
     tpe::DevBuf mat_A, mat_L, mat_Linv, mat_B, mat_B0;
     tpe::DevBuf con_C, con_Y, con_phi, con_blocks, con_ell0, con_red;
+    tpe::DevBuf con_part;  // split partial reductions of the constraint rows
     tpe::DevBuf rhs, sol, tmp, solve_scratch;
     tpe::DevBuf status;                     // device-side int flags
     tpe::DevBuf trial_raw, trial_cur;       // batched line-search trials (K x 3V each)
