@@ -35,6 +35,14 @@ sys.path.insert(0, HERE)
 METRIC = "descent steps/s at V=8192: mixed+batched vs plain FP64 GPU, at <=1e-8 rel energy err"
 
 
+# Algorithmic flops per unordered disjoint edge pair (both orders), counted from
+# the kernels' arithmetic with +, -, *, /, sqrt and rsqrt as one flop each and
+# integer powers as their multiplies: the energy (4 endpoint pairs x 60 + 9),
+# the adjoint gradient with its energy (4 x 163 + 141) and the Gram pair
+# weights with their stencil (4 x 63 + 26).
+FLOP_PER_UNORDERED_PAIR = {"energy": 249, "gradient": 793, "pair_weights": 278}
+
+
 def max_over_ranks(ms, dist, device):
     """The slowest rank's time, on every rank (ms itself without a process group)."""
     if dist is None:
@@ -529,13 +537,13 @@ def run_repulsive(args):
     steps = args.steps
     P = len(e) * (len(e) - 3)
     if dom in ("gradient", "energy", "pair_weights"):
-        fl = {"gradient": 2 * 4 * 110, "energy": 4 * 34, "pair_weights": 4 * 45}[dom]
-        per_launch_flop = P * fl
+        fl = FLOP_PER_UNORDERED_PAIR[dom]
+        per_launch_flop = P / 2 * fl
         n_launch = max(1, nl[dom] // {"gradient": 2, "energy": 2, "pair_weights": 1}[dom])
         roof = {"bound": "tensor", "unit": "TFLOP/s", "peak": fp64_peak,
                 "peak_source": "cuBLAS FP64 GEMM measured in this run (the FP64 pipe; MEASURED_PEAKS.json "
                                "lists HBM and bf16 only)",
-                "kernel": dom, "work_per_launch": f"{fl} flop x {P} ordered pairs"}
+                "kernel": dom, "work_per_launch": f"{fl} flop x {P // 2} unordered pairs"}
         achieved = per_launch_flop * n_launch / (ms_g[dom] * 1e-3) / 1e12
     elif dom == "cholesky":
         per_launch_flop = V ** 3 / 3.0
@@ -567,11 +575,13 @@ def run_repulsive(args):
     if args.precision == "mixed" and nl["gradient"] > 0:
         nsm = torch.cuda.get_device_properties(dev).multi_processor_count
         gsm = int(os.environ.get("TPE_GRAD_SMS", nsm * 2 // 5))
-        g_ach = P * 2 * 4 * 110 * max(1, nl["gradient"] // 2) / (ms_g["gradient"] * 1e-3) / 1e12
+        g_ach = P / 2 * FLOP_PER_UNORDERED_PAIR["gradient"] * max(1, nl["gradient"] // 2) / (ms_g["gradient"] * 1e-3) / 1e12
         roof["concurrent_gradient"] = {
             "sms": gsm, "achieved": g_ach, "peak_on_its_sms": fp64_peak * gsm / nsm,
             "frac": g_ach / (fp64_peak * gsm / nsm) if fp64_peak else None, "unit": "TFLOP/s",
-            "note": "adjoint gradient on stream3, bounded to `sms` SMs while the factorization runs"}
+            "note": "adjoint gradient on stream3, bounded to `sms` SMs while the factorization runs; "
+                    "the peak is the measured cuBLAS FP64 GEMM rate (DMMA), scaled to these SMs, "
+                    "while the gradient runs on the FP64 FMA pipe"}
     roof["group_pass_ms_per_step"] = ms_prof / steps
     roof["group_pass"] = ("a second pass over the same trajectory with CUDA events around each kernel "
                           "group on the launching streams; the headline ms_per_step is the pass "

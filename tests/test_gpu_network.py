@@ -6,15 +6,17 @@ barycenter + point constraints.
 The adjoint gradient (tangent-point energy + penalties) against central
 differences along 256 seeded random unit directions (h = 1e-6) with the gate of the
 reference's gradient test, |fd - an| <= 1e-6 + 1e-5 max|an|; then a descent
-trajectory in FP64 and in mixed precision (which takes the FP64 Schur path for
-a constraint set this large, so the two trajectories agree bit for bit): every
-step is accepted or reports a reason, the objective never increases, the pins
-hold and the edge lengths stay within the projection tolerance."""
+trajectory of 50 steps in FP64 and in mixed precision (which takes the FP64
+Schur path for a constraint set this large, so the two trajectories agree bit
+for bit): every step is accepted or reports a reason, the objective never
+increases, the pins hold and the edge lengths stay within the projection
+tolerance. The objective's gradient is also compared with the oracle's."""
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
+import oracle_lib as O
 from repulsive_test2_b200 import api as T
 from repulsive_test2_b200 import fixtures as F
 
@@ -58,11 +60,24 @@ def test_network_gradient_vs_central_differences(network):
     assert np.max(np.abs(fd - an)) <= 1e-6 + 1e-5 * np.max(np.abs(an))
 
 
+def test_network_gradient_vs_oracle(network):
+    """The network's objective gradient (tangent-point adjoint + penalties)
+    against the oracle's gradientAnalytical + penaltyGradient, 1e-10 relative."""
+    v, e, _ = network
+    en, g = T.energyAndGradient(v, e)
+    g = g + T.penaltyGradient(v, e, PEN)
+    pen = O.penalties_struct(1.0, 10.0, 5.0, (0.5, 1.0, 0.0))
+    want = O.gradient(v, e) + O.penalty_gradient(v, e, pen)
+    assert np.linalg.norm(g - want) <= 1e-10 * np.linalg.norm(want)
+    assert abs(en - O.energy(v, e)) <= 1e-10 * abs(en)
+
+
 def test_network_descent_fp64_and_mixed(network):
+    """Config 5's 50 descent steps in FP64 and in mixed precision."""
     v0, e, pins = network
     blocks = _blocks(v0, e, pins)
     ell0 = T.edgeLengths(v0, e)
-    nsteps = 6
+    nsteps = 50
     traj = {}
     for prec in ("fp64", "mixed"):
         v = v0.copy()
