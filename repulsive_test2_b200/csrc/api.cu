@@ -995,9 +995,9 @@ int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, c
                                          cudaMemcpyHostToDevice, ctx->stream));
             TPE_CUDA_TRY(cudaMemcpyAsync(d_coef, coef.data(), sizeof(double) * coef.size(),
                                          cudaMemcpyHostToDevice, ctx->stream));
+            // (copies from pageable host memory return once the data is staged,
+            // so the host vectors may change after them without a synchronization)
             TPE_TRY(project_update(ctx, op.Y, k, V, d_coef, nu, d_idx, d_cur, m, d_bad));
-            // the host vectors must outlive the copies
-            TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         }
     }
     return TPE_OK;
