@@ -71,7 +71,7 @@ def parse():
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of oracle work")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the per-edge, multi-curve batch and network measurements")
-    p.add_argument("--network-steps", type=int, default=10)
+    p.add_argument("--network-steps", type=int, default=50)
     return p.parse_args()
 
 
