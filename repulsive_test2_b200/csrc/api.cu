@@ -1259,6 +1259,12 @@ tpe_ctx* tpe_create(int32_t device, int32_t* status) {
         const int n = atoi(g);
         if (n >= 0) ctx->grad_sms = n;  // 0: an ordinary grid over all SMs
     }
+    // SMs the trailing updates leave to the factorization's other launches
+    ctx->free_sms = 8;
+    if (const char* g = getenv("TPE_FACTOR_FREE_SMS")) {
+        const int n = atoi(g);
+        if (n >= 0) ctx->free_sms = n;
+    }
     if (status) *status = TPE_OK;
     return ctx;
 }

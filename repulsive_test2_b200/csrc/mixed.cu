@@ -1176,7 +1176,7 @@ int32_t mixed_factor(tpe_ctx* ctx, const double* d_A, int32_t V, double rho, boo
     // The trailing updates run persistent (one CTA per SM walking its tiles) on
     // the SMs left by the concurrent gradient, minus a few kept free so that the
     // chain's launches never wait for a whole update.
-    const int32_t rest_ctas = std::max(16, ctx->num_sms - ctx->grad_sms - 8);
+    const int32_t rest_ctas = std::max(16, ctx->num_sms - ctx->grad_sms - ctx->free_sms);
     {
         const int64_t nrest = nb > 2 ? nb - 2 : 0;
         KernelScope ks(ctx, TPE_KGROUP_CHOLESKY, 2 + (int64_t)nb + (int64_t)(nb - 1) + 4 * nrest + (nrest > 0 ? nrest - 1 : 0) +

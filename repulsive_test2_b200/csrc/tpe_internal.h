@@ -124,6 +124,9 @@ struct tpe_ctx {
     // SMs the concurrent gradient may occupy; the rest stay free for the
     // factorization's chain of small launches (TPE_GRAD_SMS overrides)
     int32_t grad_sms = 0;
+    // SMs the persistent trailing updates leave free for the chain's and the
+    // panel's launches (TPE_FACTOR_FREE_SMS overrides)
+    int32_t free_sms = 8;
     std::vector<cudaEvent_t> fac_events;      // dependency events (no timing)
     std::string err;
     int32_t num_sms = 0;
