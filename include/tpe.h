@@ -289,6 +289,22 @@ int32_t tpe_energy_noalloc(const double* d_xyz, const int32_t* d_edges, int32_t 
 int32_t tpe_sobolev_step_device(tpe_ctx* ctx, const double* d_xyz, const tpe_constraint* set,
                                 int32_t nblocks, const tpe_step_opts* opts, double* d_xyz_out,
                                 tpe_step_stats* stats, double* timings);
+/* The dense FP64 product the large-constraint-set solve is built from, exposed
+ * for checking and timing (no counterpart in the reference, whose dense algebra
+ * is scalar JavaScript): C = alpha * A * B^T + beta * C with row-major device
+ * matrices A (M x K, row stride lda), B (N x K, ldb), C (M x N, ldc) on this
+ * context's device and stream. method TPE_GEMM_FP64 runs on the FP64 tensor
+ * cores; TPE_GEMM_INT8_EMULATED cuts each row into seven 8-bit digits under a
+ * power-of-two row scale and forms the exact integer digit products on the
+ * int8 tensor cores (FP64-class accuracy: error within a few units of 2^-53
+ * of max_k |A[i][k]| * max_k |B[j][k]| per term). mode: bit 0 only output
+ * tiles on or below the diagonal (M == N), bit 1/2 A upper/lower triangular
+ * (the K range skips its zeros), bits 3/4 the same for B and bit 5 writes only
+ * elements with column <= row (bits 3-5 with the integer method only). */
+enum { TPE_GEMM_FP64 = 0, TPE_GEMM_INT8_EMULATED = 1 };
+int32_t tpe_gemm_nt_device(tpe_ctx* ctx, int32_t method, int32_t M, int32_t N, int32_t K,
+                           const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                           int64_t ldc, double alpha, double beta, int32_t mode);
 /* The CUDA stream (cudaStream_t) every launch of this context is issued on. */
 void* tpe_stream(tpe_ctx* ctx);
 /* Kernel groups timed with CUDA events on that stream while profiling is on. */

@@ -42,6 +42,7 @@ DE_ANALYTICAL, DE_FINITE_DIFF = 0, 1
 PROJECTION_REASSEMBLE, PROJECTION_FROZEN = 0, 1
 FACTOR_LDLT, FACTOR_LU = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+GEMM_FP64, GEMM_INT8_EMULATED = 0, 1
 
 PHASE_KEYS = ["dE", "energy", "bHigh", "bLow", "assembleA", "expand", "saddle", "factor",
               "projection", "lineSearch", "step", "refine"]
@@ -157,6 +158,9 @@ SIGNATURES = {
                                             C.POINTER(tpe_step_opts), C.c_void_p,
                                             C.POINTER(tpe_step_stats), dp]),
     "tpe_stream": (C.c_void_p, [vp]),
+    "tpe_gemm_nt_device": (C.c_int32, [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                       C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                       C.c_double, C.c_double, C.c_int32]),
     "tpe_energy_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(tpe_params),
                                        C.c_void_p, C.c_void_p]),
     "tpe_profile": (C.c_int32, [vp, C.c_int32]),

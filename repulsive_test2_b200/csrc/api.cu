@@ -1282,7 +1282,7 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
                       &ctx->flat3, &ctx->dir, &ctx->pairM, &ctx->edge_m, &ctx->mat_A, &ctx->mat_L,
                       &ctx->mat_Linv, &ctx->mat_B, &ctx->mat_B0, &ctx->con_C, &ctx->con_Y,
-                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->con_part, &ctx->rhs,
+                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->con_part, &ctx->oz_planes, &ctx->oz_err, &ctx->rhs,
                       &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status,
                       &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
                       &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,
@@ -1785,6 +1785,41 @@ int32_t tpe_sobolev_step_device(tpe_ctx* ctx, const double* d_xyz, const tpe_con
 }
 
 void* tpe_stream(tpe_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int32_t tpe_gemm_nt_device(tpe_ctx* ctx, int32_t method, int32_t M, int32_t N, int32_t K,
+                           const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                           int64_t ldc, double alpha, double beta, int32_t mode) {
+    return guarded(ctx, [&]() -> int32_t {
+        if (!ctx) return TPE_ERR_BAD_ARG;
+        if (M < 0 || N < 0 || K <= 0 || !A || !B || !C || lda < K || ldb < K || ldc < N ||
+            (mode & ~63) != 0 || ((mode & kDLowerTiles) && M != N) ||
+            (method != TPE_GEMM_FP64 && method != TPE_GEMM_INT8_EMULATED) ||
+            (method == TPE_GEMM_FP64 && (mode & ~7) != 0)) {
+            set_error(ctx, TPE_ERR_BAD_ARG, "tpe_gemm_nt_device: bad arguments");
+            return TPE_ERR_BAD_ARG;
+        }
+        TPE_CUDA_TRY(cudaSetDevice(ctx->device));
+        DGemmArgs g;
+        g.A = A;
+        g.lda = lda;
+        g.B = B;
+        g.ldb = ldb;
+        g.C = C;
+        g.ldc = ldc;
+        g.M = M;
+        g.N = N;
+        g.K = K;
+        g.alpha = alpha;
+        g.beta = beta;
+        g.mode = mode;
+        if (method == TPE_GEMM_FP64) {
+            KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
+            return dgemm_nt(ctx, g, ctx->stream);
+        }
+        TPE_TRY(ozaki_gemm_nt(ctx, g, ctx->stream));
+        return ozaki_status(ctx, ctx->stream);
+    });
+}
 
 int32_t tpe_profile(tpe_ctx* ctx, int32_t on) {
     return guarded(ctx, [&]() -> int32_t {

@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -27,6 +28,9 @@ struct SplitMat {
     CUtensorMap map_hi, map_lo;  // 128 x 32 boxes, 128B swizzle
     bool maps_ok = false;
 };
+
+// The driver's cuTensorMapEncodeTiled (resolved once; null when unavailable).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // Encodes the tensor maps of m (host only; hi only when lo is null). Returns
 // false on failure.

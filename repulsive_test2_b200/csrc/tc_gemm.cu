@@ -960,6 +960,8 @@ bool encode(CUtensorMap* map, float* base, int32_t rows, int32_t cols, int32_t l
 
 }  // namespace
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() { return encoder(); }
+
 bool make_maps(SplitMat& m) {
     m.maps_ok = false;
     if (!m.hi || m.rows <= 0 || m.cols <= 0 || m.ld % 32 != 0 || m.cols > m.ld) return false;

@@ -149,6 +149,7 @@ struct tpe_ctx {
     // large constraint sets (schur.cu)
     tpe::DevBuf mat_Ainv, inv_X, inv_W, inv_T, sch_nz, sch_S, sch_L, sch_Linv, sch_Sinv, sch_vec;
     tpe::DevBuf ref_r, ref_x;  // residual and correction of the refinement step
+    tpe::DevBuf oz_planes, oz_err;  // digit planes and timeout flag of ozaki_gemm_nt
     tpe::DevBuf ycomb_part;    // split-over-rows partial sums of Y^T coef
     tpe::DevBuf mx_ctr;    // tile counters of the persistent trailing updates
     tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
@@ -269,7 +270,11 @@ int32_t gram_dots(tpe_ctx* ctx, const double* X, int32_t nx, const double* Y, in
 // A_rho = A + shift (every entry) into L (lower triangle copied), and trace(A) into *d_trace.
 int32_t shift_copy(tpe_ctx* ctx, const double* d_A, double* d_L, int32_t n, double shift);
 // C = alpha A B^T + beta C, FP64 row-major, on the FP64 tensor cores (dense.cu).
-enum : int32_t { kDLowerTiles = 1, kDAUpper = 2, kDALower = 4 };
+// kDBUpper, kDBLower (B[j][k] = 0 for k < j, k > j) and kDMaskUpper (write only
+// elements with column <= row) are for ozaki_gemm_nt only.
+enum : int32_t {
+    kDLowerTiles = 1, kDAUpper = 2, kDALower = 4, kDBUpper = 8, kDBLower = 16, kDMaskUpper = 32
+};
 struct DGemmArgs {
     const double* A = nullptr;
     int64_t lda = 0;
@@ -282,6 +287,16 @@ struct DGemmArgs {
     int32_t mode = 0;
 };
 int32_t dgemm_nt(tpe_ctx* ctx, const DGemmArgs& g, cudaStream_t stream);
+// The same product on the integer tensor cores (ozaki.cu): each operand row cut
+// into seven 8-bit digits under a power-of-two row scale, the digit products
+// exact int32 GEMMs, summed in FP64: FP64-class accuracy. Scratch: ctx->oz_planes
+// (ozaki_scratch_bytes); calls on one context must share one stream. A pipeline
+// timeout sets a device flag that ozaki_status reads (and clears).
+size_t ozaki_scratch_bytes(int32_t M, int32_t N, int32_t K);
+int32_t ozaki_reserve(tpe_ctx* ctx, size_t bytes);
+int32_t ozaki_gemm_nt(tpe_ctx* ctx, const DGemmArgs& g, cudaStream_t stream,
+                      int group = TPE_KGROUP_TRSV);
+int32_t ozaki_status(tpe_ctx* ctx, cudaStream_t stream);
 // out = (L L^T)^{-1}, n x n symmetric, from the Cholesky factor and its 64x64
 // diagonal-block inverses (cholesky_fp64); X, W (n x n) and Tt ((n/2 + 64)^2)
 // are scratch. X = L^{-1} by recursive halving, then out = X^T X.
