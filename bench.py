@@ -90,20 +90,32 @@ def extras(args):
     blocks = [T.barycenterBlock(T.barycenterTarget(v, e)), T.edgeLengthsBlock(ell)]
     o = {"projectionMode": "frozen", "precision": "mixed", "trials": 8,
          "energyBefore": T.calculateEnergy(v, e)}
-    T.sobolevStepSet(v, e, None, blocks, o)
-    t0 = time.perf_counter()
-    r = T.sobolevStepSet(v, e, None, blocks, o)
-    dt = time.perf_counter() - t0
     o64 = dict(o, precision="fp64", trials=1)
-    r64 = T.sobolevStepSet(v, e, None, blocks, o64)
+
+    def one_step(opts):
+        T.sobolevStepSet(v, e, None, blocks, opts)
+        best, res = None, None
+        for _ in range(2):
+            t0 = time.perf_counter()
+            res = T.sobolevStepSet(v, e, None, blocks, opts)
+            dt_ = time.perf_counter() - t0
+            best = dt_ if best is None else min(best, dt_)
+        return best, res
+
+    dt, r = one_step(o)
+    dt64, r64 = one_step(o64)
     out["per_edge"] = {
         "workload": f"random-walk knot V=E={args.V}, [barycenter, edgeLengths] (k = {len(ell) + 3}), one step",
-        "ms_per_step": dt * 1e3, "tau": r["stats"]["tau"], "saddle_residual": r["stats"]["residual"],
+        "ms_per_step": dt * 1e3, "fp64_ms_per_step": dt64 * 1e3, "speedup_vs_fp64": dt64 / dt,
+        "tau": r["stats"]["tau"], "fp64_tau": r64["stats"]["tau"],
+        "saddle_residual": r["stats"]["residual"],
         "energy_rel_err_vs_fp64": abs(r["energy"] - r64["energy"]) / abs(r64["energy"]),
         "vertices_rel_err_vs_fp64": float(np.linalg.norm(r["vertices"] - r64["vertices"]) /
                                           np.linalg.norm(r64["vertices"])),
-        "path": "explicit FP64 inverses of A_rho and of the k x k Schur complement (k > 64); the mixed "
-                "request takes the same FP64 solve"}
+        "path": "explicit inverses of A_rho and of the k x k Schur complement (k > 64): mixed = "
+                "recursive Cholesky and triangular inverse with FP64-class products on the int8 tensor "
+                "cores (seven 8-bit digits per element, exact int32 digit GEMMs); fp64 = the same on the "
+                "FP64 tensor cores (DMMA)"}
     # 64-curve batch
     curves = F.batch_curves(count=64, vmin=256, vmax=4096, seed=3)
     sets = [[T.barycenterBlock(T.barycenterTarget(cv, ce)), T.totalLengthBlock(T.totalLength(cv, ce))]
@@ -152,6 +164,7 @@ def extras(args):
                      "energy_last": rr["energy"]}
     net["mixed_vs_fp64_vertices_rel_err"] = float(np.linalg.norm(finals["mixed"] - finals["fp64"]) /
                                                   np.linalg.norm(finals["fp64"]))
+    net["speedup_vs_fp64"] = net["fp64"]["ms_per_step"] / net["mixed"]["ms_per_step"]
     out["network"] = net
     return out
 

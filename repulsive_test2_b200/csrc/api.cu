@@ -370,6 +370,7 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
     op.W = nullptr;
     op.w_src = nullptr;
     op.large = false;
+    op.int8 = false;
     op.Ainv = op.Sinv = nullptr;
     *singular = false;
     const int32_t nb = (V + kNB - 1) / kNB;
@@ -403,7 +404,8 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
             return TPE_OK;
         }
     }
-    op.Scc.assign((size_t)k * k, 0.0);
+    // (large sets keep their Schur complement on the device: no k x k host array)
+    op.Scc.assign(k > kLargeSchur ? 0 : (size_t)k * k, 0.0);
     op.Scu.assign((size_t)k * 3, 0.0);
     op.trans_constrained = false;
     // Y = Abar_rho^{-1} C^T (3k right-hand sides of length V) and, when given,
@@ -450,12 +452,18 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
     }
     if (!op.mixed) {
         TPE_TRY(shift_copy(ctx, op.A, op.L, V, rho / V));
-        int32_t bad = 0;
         const double tol = 32.0 * 2.220446049250313e-16 * (tm[1] + rho / V);
-        TPE_TRY(cholesky_fp64(ctx, op.L, op.Linv, V, tol, &bad));
-        if (bad) {
-            *singular = true;
-            return TPE_OK;
+        // mixed precision with a large set: the explicit inverses with their
+        // products on the integer tensor cores (schur.cu), no FP64 factor here
+        op.int8 = o && o->precision == TPE_PRECISION_MIXED && k > kLargeSchur;
+        op.chol_tol = tol;
+        if (!op.int8) {
+            int32_t bad = 0;
+            TPE_TRY(cholesky_fp64(ctx, op.L, op.Linv, V, tol, &bad));
+            if (bad) {
+                *singular = true;
+                return TPE_OK;
+            }
         }
         if (k > kLargeSchur) {
             // explicit inverses, Y by gathers, the Schur complement on the device
@@ -1282,7 +1290,7 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
                       &ctx->flat3, &ctx->dir, &ctx->pairM, &ctx->edge_m, &ctx->mat_A, &ctx->mat_L,
                       &ctx->mat_Linv, &ctx->mat_B, &ctx->mat_B0, &ctx->con_C, &ctx->con_Y,
-                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->con_part, &ctx->oz_planes, &ctx->oz_err, &ctx->rhs,
+                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->con_part, &ctx->oz_planes, &ctx->oz_err, &ctx->oz_base, &ctx->rhs,
                       &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status,
                       &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
                       &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,

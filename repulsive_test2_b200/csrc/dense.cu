@@ -1125,16 +1125,39 @@ int32_t inverse_blocks(tpe_ctx* ctx, const double* L, int32_t n, double* X, doub
 }
 }  // namespace
 
-int32_t spd_inverse_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
-                         double* X, double* W, double* Tt, double* out) {
+int32_t lower_inverse_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
+                           double* X, double* W, double* Tt) {
     const int32_t nb = (n + NB - 1) / NB;
     int64_t launches = 0;
-    KernelScope ks(ctx, TPE_KGROUP_TRSV, 3 + 3 * (int64_t)(nb - 1));
+    KernelScope ks(ctx, TPE_KGROUP_TRSV, 1 + 3 * (int64_t)(nb - 1));
     TPE_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n * n, ctx->stream));
     TPE_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * (size_t)n * n, ctx->stream));
     diag_inverse_kernel<<<nb, 256, 0, ctx->stream>>>(d_Linv, n, X, W);
     TPE_CUDA_TRY(cudaGetLastError());
-    TPE_TRY(inverse_blocks(ctx, d_L, n, X, W, Tt, 0, nb, &launches));
+    return inverse_blocks(ctx, d_L, n, X, W, Tt, 0, nb, &launches);
+}
+
+int32_t transpose_fp64(tpe_ctx* ctx, const double* src, int64_t lds, int32_t m, int32_t c,
+                       double* dst, int64_t ldd) {
+    KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
+    transpose_fp64_kernel<<<dim3((c + 31) / 32, (m + 31) / 32), dim3(32, 8), 0, ctx->stream>>>(
+        src, lds, m, c, dst, ldd);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
+int32_t mirror_lower(tpe_ctx* ctx, double* M, int32_t n) {
+    KernelScope ks(ctx, TPE_KGROUP_TRSV, 1);
+    const unsigned nt = (unsigned)((n + 31) / 32);
+    mirror_lower_kernel<<<dim3(nt, nt), dim3(32, 8), 0, ctx->stream>>>(M, n);
+    TPE_CUDA_TRY(cudaGetLastError());
+    return TPE_OK;
+}
+
+int32_t spd_inverse_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
+                         double* X, double* W, double* Tt, double* out) {
+    TPE_TRY(lower_inverse_fp64(ctx, d_L, d_Linv, n, X, W, Tt));
+    KernelScope ks(ctx, TPE_KGROUP_TRSV, 2);
     DGemmArgs g;  // out = X^T X = W W^T (lower tiles; W[i][k] = 0 for k < i)
     g.A = W;
     g.lda = n;

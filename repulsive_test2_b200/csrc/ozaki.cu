@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 
 #include "tpe_internal.h"
 
@@ -507,6 +508,134 @@ int32_t ozaki_status(tpe_ctx* ctx, cudaStream_t stream) {
         return TPE_ERR_DEVICE_TIMEOUT;
     }
     return TPE_OK;
+}
+
+
+// ---- SPD inverse on the integer tensor cores -------------------------------------
+
+namespace {
+
+constexpr int32_t kBase = 1024;  // largest block factored and inverted by the FP64 kernels
+
+// The base block size: kBase, or TPE_INT8_BASE (128..kBase) to test the
+// recursion at small orders.
+int32_t base_size() {
+    const char* s = getenv("TPE_INT8_BASE");
+    if (!s) return kBase;
+    const int v = atoi(s);
+    return v < 128 ? 128 : (v > kBase ? kBase : v);
+}
+
+struct InvCtx {
+    tpe_ctx* ctx;
+    double* M;  // n x n, lower triangle: A, overwritten by L below the diagonal blocks
+    double* X;  // L^{-1}, lower
+    double* W;  // X^T, upper
+    double* Tt;
+    double* base;  // kBase^2 (block) + 64 kBase (diagonal inverses) + 2 kBase^2 (X, W) + T
+    int32_t n;
+    double tol;
+    int32_t nbase;
+    bool singular;
+};
+
+DGemmArgs gemm_args(const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                    int64_t ldc, int32_t M, int32_t N, int32_t K, double alpha, double beta,
+                    int32_t mode) {
+    DGemmArgs g;
+    g.A = A;
+    g.lda = lda;
+    g.B = B;
+    g.ldb = ldb;
+    g.C = C;
+    g.ldc = ldc;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.alpha = alpha;
+    g.beta = beta;
+    g.mode = mode;
+    return g;
+}
+
+int32_t inv_base(InvCtx& c, int32_t o, int32_t m) {
+    tpe_ctx* ctx = c.ctx;
+    const cudaStream_t st = ctx->stream;
+    const int64_t n = c.n;
+    double* Bm = c.base;
+    double* Binv = Bm + (size_t)kBase * kBase;
+    double* Xb = Binv + (size_t)kBase * kNB;  // (kBase / 64) diagonal 64 x 64 inverses
+    double* Wb = Xb + (size_t)kBase * kBase;
+    double* Tb = Wb + (size_t)kBase * kBase;
+    TPE_CUDA_TRY(cudaMemcpy2DAsync(Bm, sizeof(double) * m, c.M + o * n + o, sizeof(double) * n,
+                                   sizeof(double) * m, m, cudaMemcpyDeviceToDevice, st));
+    int32_t bad = 0;
+    TPE_TRY(cholesky_fp64(ctx, Bm, Binv, m, c.tol, &bad));
+    if (bad) {
+        c.singular = true;
+        return TPE_OK;
+    }
+    TPE_TRY(lower_inverse_fp64(ctx, Bm, Binv, m, Xb, Wb, Tb));
+    TPE_CUDA_TRY(cudaMemcpy2DAsync(c.X + o * n + o, sizeof(double) * n, Xb, sizeof(double) * m,
+                                   sizeof(double) * m, m, cudaMemcpyDeviceToDevice, st));
+    TPE_CUDA_TRY(cudaMemcpy2DAsync(c.W + o * n + o, sizeof(double) * n, Wb, sizeof(double) * m,
+                                   sizeof(double) * m, m, cudaMemcpyDeviceToDevice, st));
+    return TPE_OK;
+}
+
+// Block [o, o + m) of the diagonal: L, X = L^{-1} and W = X^T, from the trailing
+// matrix held in c.M (updated by the blocks before it).
+int32_t inv_rec(InvCtx& c, int32_t o, int32_t m) {
+    if (m <= c.nbase) return inv_base(c, o, m);
+    tpe_ctx* ctx = c.ctx;
+    const cudaStream_t st = ctx->stream;
+    const int64_t n = c.n;
+    const int32_t h = (m / 2 + 63) / 64 * 64, m2 = m - h;
+    const int32_t o2 = o + h;
+    TPE_TRY(inv_rec(c, o, h));
+    if (c.singular) return TPE_OK;
+    double* A21 = c.M + o2 * n + o;
+    // L21 = A21 X11^T, in place (the product reads A21's digits, not A21)
+    TPE_TRY(ozaki_gemm_nt(ctx, gemm_args(A21, n, c.X + o * n + o, n, A21, n, m2, h, h, 1.0, 0.0,
+                                         kDBLower), st));
+    // A22 -= L21 L21^T (lower triangle)
+    TPE_TRY(ozaki_gemm_nt(ctx, gemm_args(A21, n, A21, n, c.M + o2 * n + o2, n, m2, m2, h, -1.0, 1.0,
+                                         kDLowerTiles | kDMaskUpper), st));
+    TPE_TRY(inv_rec(c, o2, m2));
+    if (c.singular) return TPE_OK;
+    // T^T (h x m2) = W11 L21^T, then X21 = -X22 T, W12 = X21^T
+    TPE_TRY(ozaki_gemm_nt(ctx, gemm_args(c.W + o * n + o, n, A21, n, c.Tt, m2, h, m2, h, 1.0, 0.0,
+                                         kDAUpper), st));
+    TPE_TRY(ozaki_gemm_nt(ctx, gemm_args(c.X + o2 * n + o2, n, c.Tt, m2, c.X + o2 * n + o, n, m2, h,
+                                         m2, -1.0, 0.0, kDALower), st));
+    TPE_TRY(transpose_fp64(ctx, c.X + o2 * n + o, n, m2, h, c.W + o * n + o2, n));
+    return TPE_OK;
+}
+
+}  // namespace
+
+int32_t spd_inverse_int8(tpe_ctx* ctx, double* Mat, int32_t n, double piv_tol, double* X,
+                         double* W, double* Tt, double* out, bool* singular) {
+    *singular = false;
+    if (n <= 0) return TPE_OK;
+    TPE_TRY(ozaki_reserve(ctx, ozaki_scratch_bytes(n, 0, n)));
+    const size_t base_doubles = (size_t)kBase * kBase * 3 + (size_t)kBase * kNB +
+                                (size_t)(kBase / 2 + kNB) * (kBase / 2 + kNB);
+    TPE_TRY(ensure(ctx, ctx->oz_base, sizeof(double) * base_doubles));
+    TPE_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double) * (size_t)n * n, ctx->stream));
+    TPE_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * (size_t)n * n, ctx->stream));
+    InvCtx c{ctx, Mat, X, W, Tt, ctx->oz_base.as<double>(), n, piv_tol, base_size(), false};
+    TPE_TRY(inv_rec(c, 0, n));
+    TPE_TRY(ozaki_status(ctx, ctx->stream));
+    if (c.singular) {
+        *singular = true;
+        return TPE_OK;
+    }
+    // out = X^T X = W W^T (lower tiles; W[i][k] = 0 for k < i), mirrored
+    TPE_TRY(ozaki_gemm_nt(ctx, gemm_args(W, n, W, n, out, n, n, n, n, 1.0, 0.0,
+                                         kDLowerTiles | kDAUpper), ctx->stream));
+    TPE_TRY(mirror_lower(ctx, out, n));
+    return ozaki_status(ctx, ctx->stream);
 }
 
 }  // namespace tpe

@@ -190,8 +190,19 @@ int32_t large_schur_build(tpe_ctx* ctx, SaddleOp& op, const double* b_flat, bool
     TPE_TRY(ensure(ctx, ctx->inv_W, sizeof(double) * nn));
     TPE_TRY(ensure(ctx, ctx->inv_T, sizeof(double) * half));
     double* Ainv = ctx->mat_Ainv.as<double>();
-    TPE_TRY(spd_inverse_fp64(ctx, op.L, op.Linv, V, ctx->inv_X.as<double>(), ctx->inv_W.as<double>(),
-                             ctx->inv_T.as<double>(), Ainv));
+    if (op.int8) {
+        // op.L holds A_rho unfactored; it is overwritten
+        bool sing = false;
+        TPE_TRY(spd_inverse_int8(ctx, op.L, V, op.chol_tol, ctx->inv_X.as<double>(),
+                                 ctx->inv_W.as<double>(), ctx->inv_T.as<double>(), Ainv, &sing));
+        if (sing) {
+            *singular = true;
+            return TPE_OK;
+        }
+    } else {
+        TPE_TRY(spd_inverse_fp64(ctx, op.L, op.Linv, V, ctx->inv_X.as<double>(),
+                                 ctx->inv_W.as<double>(), ctx->inv_T.as<double>(), Ainv));
+    }
     op.Ainv = Ainv;
     // sparse structure of C
     TPE_TRY(ensure(ctx, ctx->sch_nz, (sizeof(int32_t) + sizeof(double)) * (size_t)k * 3 * kNZ +
@@ -245,15 +256,25 @@ int32_t large_schur_build(tpe_ctx* ctx, SaddleOp& op, const double* b_flat, bool
     }
     double* Ls = ctx->sch_L.as<double>();
     TPE_CUDA_TRY(cudaMemcpyAsync(Ls, S, sizeof(double) * (size_t)k * k, cudaMemcpyDeviceToDevice, st));
-    int32_t bad = 0;
-    TPE_TRY(cholesky_fp64(ctx, Ls, ctx->sch_Linv.as<double>(), k, 0.0, &bad));
-    if (bad) {
-        *singular = true;
-        return TPE_OK;
+    if (op.int8) {
+        bool sing = false;
+        TPE_TRY(spd_inverse_int8(ctx, Ls, k, 0.0, ctx->inv_X.as<double>(), ctx->inv_W.as<double>(),
+                                 ctx->inv_T.as<double>(), ctx->sch_Sinv.as<double>(), &sing));
+        if (sing) {
+            *singular = true;
+            return TPE_OK;
+        }
+    } else {
+        int32_t bad = 0;
+        TPE_TRY(cholesky_fp64(ctx, Ls, ctx->sch_Linv.as<double>(), k, 0.0, &bad));
+        if (bad) {
+            *singular = true;
+            return TPE_OK;
+        }
+        TPE_TRY(spd_inverse_fp64(ctx, Ls, ctx->sch_Linv.as<double>(), k, ctx->inv_X.as<double>(),
+                                 ctx->inv_W.as<double>(), ctx->inv_T.as<double>(),
+                                 ctx->sch_Sinv.as<double>()));
     }
-    TPE_TRY(spd_inverse_fp64(ctx, Ls, ctx->sch_Linv.as<double>(), k, ctx->inv_X.as<double>(),
-                             ctx->inv_W.as<double>(), ctx->inv_T.as<double>(),
-                             ctx->sch_Sinv.as<double>()));
     op.Sinv = ctx->sch_Sinv.as<double>();
     return TPE_OK;
 }

@@ -72,6 +72,8 @@ struct SaddleOp {
     bool large = false;
     double* Ainv = nullptr;  // V x V: A_rho^{-1}
     double* Sinv = nullptr;  // k x k: (C A3^{-1} C^T)^{-1}
+    bool int8 = false;       // both inverses with their products on the int8 tensor cores
+    double chol_tol = 0.0;   // pivot tolerance of A_rho's Cholesky
     // host: small Schur complement and its factors
     std::vector<double> Scc;   // k x k, then its Cholesky factor (lower)
     std::vector<double> Scu;   // k x 3 = C U / rho
@@ -150,6 +152,7 @@ struct tpe_ctx {
     tpe::DevBuf mat_Ainv, inv_X, inv_W, inv_T, sch_nz, sch_S, sch_L, sch_Linv, sch_Sinv, sch_vec;
     tpe::DevBuf ref_r, ref_x;  // residual and correction of the refinement step
     tpe::DevBuf oz_planes, oz_err;  // digit planes and timeout flag of ozaki_gemm_nt
+    tpe::DevBuf oz_base;            // the FP64 base blocks of spd_inverse_int8
     tpe::DevBuf ycomb_part;    // split-over-rows partial sums of Y^T coef
     tpe::DevBuf mx_ctr;    // tile counters of the persistent trailing updates
     tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
@@ -302,6 +305,23 @@ int32_t ozaki_status(tpe_ctx* ctx, cudaStream_t stream);
 // are scratch. X = L^{-1} by recursive halving, then out = X^T X.
 int32_t spd_inverse_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
                          double* X, double* W, double* Tt, double* out);
+// X = L^{-1} (lower) and W = X^T (upper), n x n, from the Cholesky factor and its
+// 64x64 diagonal-block inverses (the first half of spd_inverse_fp64).
+int32_t lower_inverse_fp64(tpe_ctx* ctx, const double* d_L, const double* d_Linv, int32_t n,
+                           double* X, double* W, double* Tt);
+// M[j][i] = M[i][j] for j > i (n x n, row-major).
+int32_t mirror_lower(tpe_ctx* ctx, double* M, int32_t n);
+// dst[j][i] = src[i][j] for an m x c block (row strides lds, ldd).
+int32_t transpose_fp64(tpe_ctx* ctx, const double* src, int64_t lds, int32_t m, int32_t c,
+                       double* dst, int64_t ldd);
+// out = A^{-1} for the SPD n x n matrix in Mat (lower triangle read; Mat is
+// overwritten) with the heavy products on the integer tensor cores
+// (ozaki_gemm_nt): recursive Cholesky and triangular inverse in halves down to
+// blocks of at most 1024 (cholesky_fp64 + lower_inverse_fp64 there), then
+// out = X^T X. X, W (n x n) and Tt ((n/2 + 64)^2) are scratch. A pivot at or
+// below piv_tol sets *singular.
+int32_t spd_inverse_int8(tpe_ctx* ctx, double* Mat, int32_t n, double piv_tol, double* X,
+                         double* W, double* Tt, double* out, bool* singular);
 // Y[c][i] = sum_j M[i][j] X[c][j] for c < nr <= 16: M n x n FP64 (row length n),
 // X and Y nr rows of stride ldx >= n (mixed.cu: the CG's multi-RHS kernel).
 int32_t mrhs_fp64(tpe_ctx* ctx, const double* M, int32_t n, const double* X, int32_t ldx,
