@@ -114,7 +114,7 @@ def extras(args):
                                           np.linalg.norm(r64["vertices"])),
         "path": "explicit inverses of A_rho and of the k x k Schur complement (k > 64): mixed = "
                 "recursive Cholesky and triangular inverse with FP64-class products on the int8 tensor "
-                "cores (seven 8-bit digits per element, exact int32 digit GEMMs); fp64 = the same on the "
+                "cores (eight 8-bit digits per element, exact int32 digit GEMMs); fp64 = the same on the "
                 "FP64 tensor cores (DMMA)"}
     # 64-curve batch
     curves = F.batch_curves(count=64, vmin=256, vmax=4096, seed=3)

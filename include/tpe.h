@@ -294,7 +294,7 @@ int32_t tpe_sobolev_step_device(tpe_ctx* ctx, const double* d_xyz, const tpe_con
  * is scalar JavaScript): C = alpha * A * B^T + beta * C with row-major device
  * matrices A (M x K, row stride lda), B (N x K, ldb), C (M x N, ldc) on this
  * context's device and stream. method TPE_GEMM_FP64 runs on the FP64 tensor
- * cores; TPE_GEMM_INT8_EMULATED cuts each row into seven 8-bit digits under a
+ * cores; TPE_GEMM_INT8_EMULATED cuts each row into eight 8-bit digits under a
  * power-of-two row scale and forms the exact integer digit products on the
  * int8 tensor cores (FP64-class accuracy: error within a few units of 2^-53
  * of max_k |A[i][k]| * max_k |B[j][k]| per term). mode: bit 0 only output

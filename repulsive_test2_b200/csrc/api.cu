@@ -455,7 +455,8 @@ int32_t op_finalize(tpe_ctx* ctx, int32_t V, int32_t k, bool* singular,
         const double tol = 32.0 * 2.220446049250313e-16 * (tm[1] + rho / V);
         // mixed precision with a large set: the explicit inverses with their
         // products on the integer tensor cores (schur.cu), no FP64 factor here
-        op.int8 = o && o->precision == TPE_PRECISION_MIXED && k > kLargeSchur;
+        op.int8 = o && o->precision == TPE_PRECISION_MIXED && k > kLargeSchur &&
+                  o->projection_mode == TPE_PROJECTION_FROZEN;
         op.chol_tol = tol;
         if (!op.int8) {
             int32_t bad = 0;
@@ -727,6 +728,8 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
     const int64_t m = 3 * (int64_t)V;
     TPE_TRY(op_solve_once(ctx, b_flat, d, x_flat, lam));
     if (op.large && b_flat && k > 0) {
+        // iterative refinement on the FP64 residual until it reaches kRefineStop,
+        // stops shrinking by half, or kLargeRefineMax corrections are made
         TPE_TRY(ensure(ctx, ctx->ref_r, sizeof(double) * (size_t)m));
         TPE_TRY(ensure(ctx, ctx->ref_x, sizeof(double) * (size_t)m));
         double* rt = ctx->ref_r.as<double>();
@@ -734,12 +737,22 @@ int32_t op_solve(tpe_ctx* ctx, const double* b_flat, const double* d, double* x_
         std::vector<double> bottom((size_t)k, 0.0), rb((size_t)k, 0.0), dlam;
         if (d)
             for (int32_t r = 0; r < k; r++) bottom[r] = d[r];
-        double r0 = 0.0;
-        TPE_TRY(saddle_residual(ctx, op.A, V, op.C, k, x_flat, lam.data(), b_flat, bottom.data(),
-                                &r0, rt, rb.data()));
-        TPE_TRY(op_solve_once(ctx, rt, rb.data(), dx, dlam));
-        TPE_TRY(axpby(ctx, m, 1.0, dx, 1.0, x_flat));
-        for (int32_t r = 0; r < k; r++) lam[r] += dlam[r];
+        double prev = 0.0;
+        for (int32_t it = 0;; it++) {
+            double r0 = 0.0;
+            TPE_TRY(saddle_residual(ctx, op.A, V, op.C, k, x_flat, lam.data(), b_flat, bottom.data(),
+                                    &r0, rt, rb.data()));
+            const bool done = it > 0 && (!(r0 > kRefineStop) || !(r0 < 0.5 * prev) ||
+                                         it >= kLargeRefineMax);
+            if (done) {
+                if (residual) *residual = r0;
+                return TPE_OK;
+            }
+            prev = r0;
+            TPE_TRY(op_solve_once(ctx, rt, rb.data(), dx, dlam));
+            TPE_TRY(axpby(ctx, m, 1.0, dx, 1.0, x_flat));
+            for (int32_t r = 0; r < k; r++) lam[r] += dlam[r];
+        }
     }
     if (residual) {
         const double* top = b_flat;
@@ -1690,23 +1703,49 @@ int32_t step_impl(tpe_ctx* ctx, const tpe_constraint* set, int32_t nblocks, cons
     const int32_t fst = finish_gradient(ctx);  // joined even when the build returned early
     TPE_TRY(bst);
     TPE_TRY(fst);
-    st->refine_iterations = ctx->op.mixed ? ctx->op.refine_iters : (ctx->op.mixed_fallback ? -1 : 0);
+    // The mixed mode's int8-tensor-core inverses (large constraint sets) are
+    // rebuilt in FP64 when they come out singular or when the refined gradient
+    // solve misses kInt8ResidualGate: conditioning that the digit products do
+    // not resolve. The step is then the FP64 step.
+    auto fallback_fp64 = [&]() -> int32_t {
+        tpe_step_opts o64 = *o;
+        o64.precision = TPE_PRECISION_FP64;
+        singular = false;
+        {
+            Timer t(ctx, timings, TPE_PHASE_FACTOR);
+            TPE_TRY(op_finalize(ctx, V, S.k, &singular, ctx->flat2.as<double>(), &o64));
+        }
+        ctx->op.mixed_fallback = true;
+        return TPE_OK;
+    };
+    if (singular && ctx->op.int8) TPE_TRY(fallback_fp64());
     TPE_TRY(ensure(ctx, ctx->sol, sizeof(double) * m));
     double* out = ctx->sol.as<double>();
+    std::vector<double> lam;
+    double res = 0.0;
+    if (!singular) {
+        TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
+        TPE_TRY(ensure(ctx, ctx->rhs, sizeof(double) * m));
+        {
+            Timer t(ctx, timings, TPE_PHASE_SADDLE);
+            TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), nullptr, ctx->flat1.as<double>(), lam, &res));
+        }
+        if (ctx->op.int8 && !(res <= kInt8ResidualGate)) {
+            TPE_TRY(fallback_fp64());
+            if (!singular) {
+                Timer t(ctx, timings, TPE_PHASE_SADDLE);
+                TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), nullptr, ctx->flat1.as<double>(), lam,
+                                 &res));
+            }
+        }
+    }
+    st->refine_iterations = ctx->op.mixed ? ctx->op.refine_iters : (ctx->op.mixed_fallback ? -1 : 0);
     if (singular) {
         double e = o->energy_before;
         if (!o->has_energy_before) TPE_TRY(objective(ctx, P, o, pen, &e, timings));
         st->energy = st->energy_before = e;
         st->reason = TPE_REASON_SINGULAR_SYSTEM;
         return TPE_OK;
-    }
-    TPE_TRY(ensure(ctx, ctx->flat1, sizeof(double) * m));
-    TPE_TRY(ensure(ctx, ctx->rhs, sizeof(double) * m));
-    std::vector<double> lam;
-    double res = 0.0;
-    {
-        Timer t(ctx, timings, TPE_PHASE_SADDLE);
-        TPE_TRY(op_solve(ctx, ctx->flat2.as<double>(), nullptr, ctx->flat1.as<double>(), lam, &res));
     }
     double* g = ctx->rhs.as<double>();
     TPE_TRY(block_to_interleaved(ctx, ctx->flat1.as<double>(), g, V));

@@ -3,18 +3,22 @@
 // C = alpha * A * B^T + beta * C for row-major FP64 A (M x K), B (N x K) and C.
 // Each row of an operand is scaled by its own power of two, 2^e with every
 // |x| < 2^e, and cut into kS 8-bit digits:
-//     x = 2^e * (d0 * 2^-7 + d1 * 2^-15 + d2 * 2^-23 + ... ) + r,  |r| < 2^(e-55),
+//     x = 2^e * (d0 * 2^-7 + d1 * 2^-15 + d2 * 2^-23 + ... ) + r,  |r| < 2^(e-63),
 // d0 signed (-128..127), d1.. unsigned (0..255). Every step of the cut (scaling
 // by a power of two, floor, subtraction) is exact in FP64. A digit product
 // d^A_p (d^B_q)^T is an exact integer GEMM (tcgen05.mma kind::i8, int32
 // accumulator in tensor memory). Products of equal level g = p + q share one
 // accumulator, since they carry the same weight 2^-(14 + 8g); levels g < kS are
-// formed (28 digit products for kS = 7), the rest lie below 2^-55 of the row
+// formed (36 digit products for kS = 8), the rest lie below 2^-63 of the row
 // scales and are dropped. The epilogue adds the level sums in FP64, smallest
 // weight first, and applies 2^(e_i + e_j), alpha and beta. The result matches
 // an FP64 GEMM to within a few units of 2^-53 of max_k |a_ik| * max_k |b_jk|
 // per term: FP64-class accuracy from the int8 tensor cores, which run at
-// several times the FP64 tensor-core rate.
+// several times the FP64 tensor-core rate. The bound is normwise per row: an
+// entry 2^-d below its row's largest keeps 63 - d bits, so where the rows'
+// entries span many orders of magnitude and the sum cancels, the product is
+// less accurate than an FP64 GEMM (the large-set solve checks its residual and
+// falls back to FP64 there).
 //
 // Int32 level sums are exact while K * kS * 255^2 < 2^31: one launch covers at
 // most kMaxK = 4096 columns of K; longer products run as several launches that
@@ -23,8 +27,8 @@
 // Pipeline: one CTA per 128 x 64 output tile (four warps). One thread issues
 // the TMA loads of all kS digit planes of A (128 x 64 bytes each) and B
 // (64 x 64 bytes each) for a 64-column K stage into a two-stage ring (64B
-// swizzle); one thread issues the 28 x 2 MMAs of a stage (M=128, N=64, K=32)
-// into the kS level accumulators (kS x 64 of the 512 TMEM columns); then all
+// swizzle); one thread issues the 36 x 2 MMAs of a stage (M=128, N=64, K=32)
+// into the kS level accumulators (all 512 TMEM columns); then all
 // four warps read the accumulators back (tcgen05.ld) and write C. Every barrier
 // wait is bounded (about 2 s): on a timeout the kernel raises *err, lets the
 // copies it issued land, frees its tensor memory and returns.
@@ -40,7 +44,7 @@ namespace tpe {
 namespace oz {
 namespace {
 
-constexpr int kS = 7;                       // digits per element
+constexpr int kS = 8;                       // digits per element
 constexpr int kBM = 128, kBN = 64;          // output tile
 constexpr int kBK = 64;                     // K digits (bytes) per stage: one 64B swizzle row
 constexpr int kStages = 2;

@@ -291,7 +291,7 @@ struct DGemmArgs {
 };
 int32_t dgemm_nt(tpe_ctx* ctx, const DGemmArgs& g, cudaStream_t stream);
 // The same product on the integer tensor cores (ozaki.cu): each operand row cut
-// into seven 8-bit digits under a power-of-two row scale, the digit products
+// into eight 8-bit digits under a power-of-two row scale, the digit products
 // exact int32 GEMMs, summed in FP64: FP64-class accuracy. Scratch: ctx->oz_planes
 // (ozaki_scratch_bytes); calls on one context must share one stream. A pipeline
 // timeout sets a device flag that ozaki_status reads (and clears).
@@ -341,6 +341,17 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
 // ---- large constraint sets (schur.cu) ----------------------------------------
 // Constraint sets with more rows than this take the explicit-inverse Schur path.
 constexpr int32_t kLargeSchur = 64;
+// Iterative refinement of the large-set gradient solve: stop at this relative
+// saddle residual, or after kLargeRefineMax corrections, or when a correction
+// no longer halves the residual.
+constexpr double kRefineStop = 1e-13;
+constexpr int32_t kLargeRefineMax = 4;
+// The refined gradient-solve residual the int8-tensor-core inverses must reach;
+// above it the step rebuilds them in FP64. The FP64 inverses reach 1e-14 after
+// one or two corrections on every measured curve; the int8 ones either do the
+// same or stall far above this (rows whose entries span many orders of
+// magnitude lose digits under a per-row scale).
+constexpr double kInt8ResidualGate = 1e-12;
 // From the FP64 factor op.L: op.Ainv, op.Y (k x 3V), op.W = A3^{-1} b when b is
 // given, and op.Sinv; *singular when the Schur complement is not SPD.
 int32_t large_schur_build(tpe_ctx* ctx, SaddleOp& op, const double* b_flat, bool* singular);

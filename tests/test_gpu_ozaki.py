@@ -20,12 +20,12 @@ from repulsive_test2_b200 import api as T
 
 pytestmark = pytest.mark.gpu
 
-S = 7
+S = 8
 MAX_K = 4096
 
 
 def split_np(X):
-    """Row scales e (|x| < 2^e) and the seven digits of each element."""
+    """Row scales e (|x| < 2^e) and the eight digits of each element."""
     m = np.max(np.abs(X), axis=1)
     e = np.where(m > 0, np.frexp(m)[1], 0).astype(np.int64)
     y = np.ldexp(X, (7 - e)[:, None])
