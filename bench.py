@@ -166,6 +166,26 @@ def extras(args):
                                                   np.linalg.norm(finals["fp64"]))
     net["speedup_vs_fp64"] = net["fp64"]["ms_per_step"] / net["mixed"]["ms_per_step"]
     out["network"] = net
+    # Barnes-Hut energy (the hierarchical path) against the exact GPU energy on a
+    # smooth curve far larger than the step's V
+    bh = {"workload": "closed trefoil (the stage-2 oracle's check curve), theta 0.5, theta_t 0.75, leaf 8; "
+                      "wall time of the public call (tree built on the host, traversal on the device)"}
+    for n in (32768, 131072):
+        tt = np.linspace(0.0, 2.0 * np.pi, n, endpoint=False)
+        tv = np.stack([np.sin(tt) + 2.0 * np.sin(2.0 * tt), np.cos(tt) - 2.0 * np.cos(2.0 * tt),
+                       -np.sin(3.0 * tt)], axis=1) * 0.25
+        te = np.stack([np.arange(n), (np.arange(n) + 1) % n], axis=1).astype(np.int32)
+        T.calculateEnergy(tv, te)
+        t0 = time.perf_counter()
+        ex = T.calculateEnergy(tv, te)
+        t_ex = time.perf_counter() - t0
+        T.bhEnergy(tv, te, theta=0.5, leafSize=8, thetaT=0.75)
+        t0 = time.perf_counter()
+        eb, stb = T.bhEnergy(tv, te, theta=0.5, leafSize=8, thetaT=0.75)
+        t_bh = time.perf_counter() - t0
+        bh[f"E{n}"] = {"exact_ms": t_ex * 1e3, "bh_ms": t_bh * 1e3, "rel_err": abs(eb - ex) / abs(ex),
+                       "direct_pairs_fraction": stb["direct_pairs"] / float(n) ** 2, **stb}
+    out["bh"] = bh
     return out
 
 

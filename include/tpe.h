@@ -254,6 +254,16 @@ int32_t tpe_step_batch(tpe_batch* batch, const double* const* xyz,
                        const tpe_step_opts* opts, double* const* xyz_out, tpe_step_stats* stats,
                        int32_t* status, int32_t max_threads);
 
+/* Barnes-Hut energy for curves far beyond the dense kernels' sizes: the
+ * reference's stage-2 oracle bh_energy (oracle/tpe_stage2_oracle.py:532-589),
+ * same tree (build_edge_bvh :467-502, built on the host), same admissibility
+ * (a node of >= 2 edges sharing no vertex with the target edge, node radius /
+ * distance <= theta, tangent radius <= theta_t; theta_t < 0 means 1.5 theta)
+ * and cluster term. theta = 0 gives the exact energy. stats (nullable, 3):
+ * tree visits, approximated edge references, exactly summed pairs. */
+int32_t tpe_energy_bh(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double theta,
+                      double theta_t, int32_t leaf_size, double* energy, int64_t* stats);
+
 /* Energies of `ncurves` curves that share this context's topology (e.g. the K
  * tau-trial candidates of one line search) in one launch: xyz is
  * ncurves x V x 3, energies[ncurves]. */

@@ -154,6 +154,8 @@ SIGNATURES = {
     "tpe_penalty_energy": (C.c_int32, [vp, dp, C.POINTER(tpe_penalties), dp]),
     "tpe_penalty_gradient": (C.c_int32, [vp, dp, C.POINTER(tpe_penalties), dp]),
     "tpe_energy_batch": (C.c_int32, [vp, dp, C.c_int32, C.POINTER(tpe_params), C.c_int32, dp]),
+    "tpe_energy_bh": (C.c_int32, [vp, dp, C.POINTER(tpe_params), C.c_double, C.c_double, C.c_int32, dp,
+                                  C.POINTER(C.c_int64)]),
     "tpe_sobolev_step_device": (C.c_int32, [vp, C.c_void_p, C.POINTER(tpe_constraint), C.c_int32,
                                             C.POINTER(tpe_step_opts), C.c_void_p,
                                             C.POINTER(tpe_step_stats), dp]),

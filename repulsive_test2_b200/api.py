@@ -173,6 +173,22 @@ def energyBatch(curves: np.ndarray, edges, alpha=3.0, beta=6.0, epsilon=1e-10) -
     return out
 
 
+def bhEnergy(vertices, edges, alpha=3.0, beta=6.0, epsilon=1e-10, theta=0.5, leafSize=8,
+             thetaT=None):
+    """Barnes-Hut energy, the stage-2 oracle's bh_energy (oracle/tpe_stage2_oracle.py:532-589):
+    (energy, {"visits", "approximated_edge_refs", "direct_pairs"}). thetaT defaults to
+    1.5 * theta; theta = 0 is the exact energy."""
+    ctx = context()
+    v = _v(vertices)
+    ctx.topology(v, edges)
+    out = C.c_double(0.0)
+    st = (C.c_int64 * 3)()
+    ctx.check(ctx.lib.tpe_energy_bh(ctx.ptr, _dp(v), C.byref(_params(alpha, beta, epsilon)), float(theta),
+                                    -1.0 if thetaT is None else float(thetaT), int(leafSize),
+                                    C.byref(out), st), "bhEnergy")
+    return out.value, {"visits": int(st[0]), "approximated_edge_refs": int(st[1]), "direct_pairs": int(st[2])}
+
+
 # ---- innerProduct.ts --------------------------------------------------------------
 
 def _assemble(vertices, edges, which, alpha, beta, epsilon):

@@ -1303,7 +1303,7 @@ void tpe_destroy(tpe_ctx* ctx) {
                       &ctx->partial, &ctx->scalars, &ctx->flat0, &ctx->flat1, &ctx->flat2,
                       &ctx->flat3, &ctx->dir, &ctx->pairM, &ctx->edge_m, &ctx->mat_A, &ctx->mat_L,
                       &ctx->mat_Linv, &ctx->mat_B, &ctx->mat_B0, &ctx->con_C, &ctx->con_Y,
-                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->con_part, &ctx->oz_planes, &ctx->oz_err, &ctx->oz_base, &ctx->rhs,
+                      &ctx->con_phi, &ctx->con_blocks, &ctx->con_ell0, &ctx->con_red, &ctx->con_part, &ctx->oz_planes, &ctx->oz_err, &ctx->oz_base, &ctx->bh_buf, &ctx->rhs,
                       &ctx->sol, &ctx->tmp, &ctx->solve_scratch, &ctx->status,
                       &ctx->trial_raw, &ctx->trial_cur, &ctx->mx_d, &ctx->mx_dinv, &ctx->mx_S,
                       &ctx->mx_Lhi, &ctx->mx_Llo, &ctx->mx_Zhi, &ctx->mx_Zlo, &ctx->mx_Whi,
@@ -1403,6 +1403,17 @@ int32_t tpe_energy(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double*
         if (!xyz || !p || !energy) return TPE_ERR_BAD_ARG;
         TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)ctx->V));
         return energy_of(ctx, ctx->pos.as<double>(), p->alpha, p->beta, p->epsilon, energy);
+    });
+}
+
+int32_t tpe_energy_bh(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double theta,
+                      double theta_t, int32_t leaf_size, double* energy, int64_t* stats) {
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !p || !energy) return TPE_ERR_BAD_ARG;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)ctx->V));
+        return bh_energy(ctx, xyz, ctx->pos.as<double>(), p->alpha, p->beta, p->epsilon, theta,
+                         theta_t < 0.0 ? 1.5 * theta : theta_t, leaf_size, energy, stats);
     });
 }
 

@@ -153,6 +153,7 @@ struct tpe_ctx {
     tpe::DevBuf ref_r, ref_x;  // residual and correction of the refinement step
     tpe::DevBuf oz_planes, oz_err;  // digit planes and timeout flag of ozaki_gemm_nt
     tpe::DevBuf oz_base;            // the FP64 base blocks of spd_inverse_int8
+    tpe::DevBuf bh_buf;             // Barnes-Hut tree, permutation and per-edge sums (bh.cu)
     tpe::DevBuf ycomb_part;    // split-over-rows partial sums of Y^T coef
     tpe::DevBuf mx_ctr;    // tile counters of the persistent trailing updates
     tpe::DevBuf pairM;                      // E x E double2 (Mb, M0) pair matrix
@@ -246,6 +247,13 @@ int32_t energy_fp64_scratch(cudaStream_t stream, const double* d_pos, const int2
 // bounds the SMs the pair kernel occupies (one block per SM).
 int32_t energy_grad_fp64(tpe_ctx* ctx, double alpha, double beta, double eps, double* d_energy,
                          double* d_grad, int32_t max_blocks = 0);
+
+// Barnes-Hut energy (bh.cu) of this context's curve: h_xyz (host) builds the
+// tree, d_xyz (device, the same positions) is traversed. stats (nullable):
+// visits, approximated edge references, direct pairs.
+int32_t bh_energy(tpe_ctx* ctx, const double* h_xyz, const double* d_xyz, double alpha, double beta,
+                  double eps, double theta, double theta_t, int32_t leaf, double* energy,
+                  int64_t* stats);
 
 // ---- mixed precision energy (pair_mixed.cu) ----------------------------------
 // FP32 pair terms, FP64 sums: tpe_energy_batch with TPE_PRECISION_MIXED only.

@@ -1,0 +1,81 @@
+"""Regenerates tests/golden/bh_cases.npz: Barnes-Hut energies of the reference's
+own stage-2 oracle (oracle/tpe_stage2_oracle.py bh_energy) with its counts.
+
+Run where a checkout of the reference repository exists, naming its root in
+REFERENCE_ROOT (required; there is no default); the GPU tests only read the
+file this writes:
+
+    REFERENCE_ROOT=<reference checkout> python tests/golden/make_bh.py
+
+Cases: the closed trefoil of the oracle's own check script (oracle/check_bh_stage2.py:
+N points on t in [0, 2 pi), scale 0.25) at N = 60 with theta = 0 (leaf 2 and 8:
+the exact energy, no cluster admitted) and at N = 120 with (theta, theta_t,
+leaf) = (0.5, 0.75, 4) and (0.25, 0.5, 4); a seeded random-walk knot (V = 512)
+at the default (0.5, 0.75, 8) and at (0.5, 0.75, 4); and a small loop network
+(3 loops of 64 joined at 2 junctions: vertices of degree 3, not one closed loop).
+Each case stores vertices, edges, (alpha, beta, epsilon, theta, theta_t, leaf),
+the energy, the exact energy (calculate_energy) and the counts (visits,
+approximated edge references, direct pairs).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("REFERENCE_ROOT", "")
+sys.path.insert(0, REPO)
+
+from repulsive_test2_b200 import fixtures  # noqa: E402
+
+ALPHA, BETA, EPS = 3.0, 6.0, 1e-10
+
+
+def trefoil(n):
+    t = np.linspace(0.0, 2.0 * np.pi, n, endpoint=False)
+    v = np.stack([np.sin(t) + 2.0 * np.sin(2.0 * t), np.cos(t) - 2.0 * np.cos(2.0 * t), -np.sin(3.0 * t)],
+                 axis=1) * 0.25
+    e = np.asarray([[i, (i + 1) % n] for i in range(n)], dtype=np.int64)
+    return v, e
+
+
+def main():
+    if not REF:
+        sys.exit("set REFERENCE_ROOT to the reference checkout")
+    sys.path.insert(0, os.path.join(REF, "oracle"))
+    import tpe_stage2_oracle as O
+
+    v60, e60 = trefoil(60)
+    v120, e120 = trefoil(120)
+    vrw, erw = fixtures.random_walk_knot(512, seed=3)
+    vnet, enet = fixtures.loop_network(loops=3, n=64, junctions=2, seed=7)
+    cases = [
+        ("trefoil60_exact_leaf2", v60, e60, 0.0, 0.0, 2),
+        ("trefoil60_exact_leaf8", v60, e60, 0.0, 0.0, 8),
+        ("trefoil120_0.5", v120, e120, 0.5, 0.75, 4),
+        ("trefoil120_0.25", v120, e120, 0.25, 0.5, 4),
+        ("walk512_default", vrw, erw, 0.5, 0.75, 8),
+        ("walk512_leaf4", vrw, erw, 0.5, 0.75, 4),
+        ("network_0.5", vnet, enet, 0.5, 0.75, 4),
+    ]
+    out = {}
+    for name, v, e, th, tht, leaf in cases:
+        v = np.asarray(v, dtype=np.float64)
+        e = np.asarray(e, dtype=np.int64)
+        en, st = O.bh_energy(v, e, ALPHA, BETA, EPS, theta=th, leaf_size=leaf, theta_t=tht)
+        ex = O.calculate_energy(v, e, ALPHA, BETA, EPS)
+        out[name + "/vertices"] = v
+        out[name + "/edges"] = e.astype(np.int32)
+        out[name + "/params"] = np.array([ALPHA, BETA, EPS, th, tht, leaf], dtype=np.float64)
+        out[name + "/energy"] = np.array([en, ex])
+        out[name + "/stats"] = np.array([st["visits"], st["approximated_edge_refs"], st["direct_pairs"]],
+                                        dtype=np.int64)
+        print(f"{name}: E={len(e)} bh={en:.17g} exact={ex:.17g} rel={abs(en - ex) / abs(ex):.2e} {st}")
+    np.savez_compressed(os.path.join(HERE, "bh_cases.npz"), **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,67 @@
+"""The Barnes-Hut energy (tpe_energy_bh), the hierarchical path of the
+reference's stage-2 oracle (oracle/tpe_stage2_oracle.py bh_energy).
+
+Against the oracle's own outputs (tests/golden/bh_cases.npz, written by
+tests/golden/make_bh.py from the reference's Python oracle): the energy within
+1e-12 and the tree visits, approximated edge references and direct pairs
+exactly, which pins the tree (same splits, same order) and every admissibility
+decision. Then the oracle check script's gates (oracle/check_bh_stage2.py) at
+sizes the Python oracle cannot reach: theta = 0 is the exact energy, clusters
+are admitted, and the error shrinks with theta."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from repulsive_test2_b200 import api as T
+from repulsive_test2_b200 import fixtures as F
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bh_cases.npz")
+
+
+def _cases():
+    z = np.load(GOLDEN)
+    names = sorted({k.split("/")[0] for k in z.files})
+    return [(n, z) for n in names]
+
+
+@pytest.mark.parametrize("name", [n for n, _ in _cases()])
+def test_bh_matches_reference_oracle(name):
+    z = np.load(GOLDEN)
+    v, e = z[name + "/vertices"], z[name + "/edges"]
+    alpha, beta, eps, th, tht, leaf = z[name + "/params"]
+    want, exact = z[name + "/energy"]
+    st_want = z[name + "/stats"]
+    got, st = T.bhEnergy(v, e, alpha, beta, eps, theta=th, leafSize=int(leaf), thetaT=tht)
+    assert abs(got - want) <= 1e-12 * abs(want), (got, want)
+    assert [st["visits"], st["approximated_edge_refs"], st["direct_pairs"]] == list(st_want)
+    if th == 0.0:
+        assert st["approximated_edge_refs"] == 0
+        assert abs(got - T.calculateEnergy(v, e)) <= 1e-12 * abs(exact)
+
+
+def test_bh_gates_at_large_sizes():
+    """check_bh_stage2.py's three gates on curves of 2048 and 16384 edges."""
+    v, e = F.random_walk_knot(2048, seed=4)
+    exact = T.calculateEnergy(v, e)
+    for leaf in (2, 8):
+        got, st = T.bhEnergy(v, e, theta=0.0, leafSize=leaf)
+        assert st["approximated_edge_refs"] == 0
+        assert abs(got - exact) <= 1e-12 * abs(exact)
+    n = 16384
+    t = np.linspace(0.0, 2.0 * np.pi, n, endpoint=False)
+    v = np.stack([np.sin(t) + 2.0 * np.sin(2.0 * t), np.cos(t) - 2.0 * np.cos(2.0 * t), -np.sin(3.0 * t)],
+                 axis=1) * 0.25
+    e = np.asarray([[i, (i + 1) % n] for i in range(n)], dtype=np.int32)
+    exact = T.calculateEnergy(v, e)
+    e05, st05 = T.bhEnergy(v, e, theta=0.5, leafSize=8, thetaT=0.75)
+    e025, st025 = T.bhEnergy(v, e, theta=0.25, leafSize=8, thetaT=0.5)
+    rel05, rel025 = abs(e05 - exact) / abs(exact), abs(e025 - exact) / abs(exact)
+    assert st05["approximated_edge_refs"] > 0
+    assert rel05 <= 5e-2 and rel025 <= rel05
+    # the tree replaces most of the n^2 pairs
+    assert st05["direct_pairs"] < 0.1 * n * n
