@@ -169,7 +169,8 @@ def extras(args):
     # Barnes-Hut energy (the hierarchical path) against the exact GPU energy on a
     # smooth curve far larger than the step's V
     bh = {"workload": "closed trefoil (the stage-2 oracle's check curve), theta 0.5, theta_t 0.75, leaf 8; "
-                      "wall time of the public call (tree built on the host, traversal on the device)"}
+                      "wall time of the public calls (tree and block lists built on the host, traversal and "
+                      "products on the device); bct_high: the high-order kernel product against theta = 0"}
     for n in (32768, 131072):
         tt = np.linspace(0.0, 2.0 * np.pi, n, endpoint=False)
         tv = np.stack([np.sin(tt) + 2.0 * np.sin(2.0 * tt), np.cos(tt) - 2.0 * np.cos(2.0 * tt),
@@ -185,6 +186,19 @@ def extras(args):
         t_bh = time.perf_counter() - t0
         bh[f"E{n}"] = {"exact_ms": t_ex * 1e3, "bh_ms": t_bh * 1e3, "rel_err": abs(eb - ex) / abs(ex),
                        "direct_pairs_fraction": stb["direct_pairs"] / float(n) ** 2, **stb}
+        if n == 32768:
+            # the block-cluster-tree product of the high-order kernel against theta = 0 (exact)
+            psi = np.sin(np.arange(n) * 0.61) + 0.2
+            t0 = time.perf_counter()
+            k_ex, _ = T.bctMatvec(tv, te, psi, "high", theta=0.0, leafSize=8)
+            t_kex = time.perf_counter() - t0
+            T.bctMatvec(tv, te, psi, "high", theta=0.5, leafSize=8, thetaT=0.75)
+            t0 = time.perf_counter()
+            k_bct, stk = T.bctMatvec(tv, te, psi, "high", theta=0.5, leafSize=8, thetaT=0.75)
+            t_k = time.perf_counter() - t0
+            bh[f"E{n}"]["bct_high"] = {"exact_ms": t_kex * 1e3, "bct_ms": t_k * 1e3,
+                                       "rel_err": float(np.linalg.norm(k_bct - k_ex) / np.linalg.norm(k_ex)),
+                                       **stk}
     out["bh"] = bh
     return out
 

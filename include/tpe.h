@@ -264,6 +264,21 @@ int32_t tpe_step_batch(tpe_batch* batch, const double* const* xyz,
 int32_t tpe_energy_bh(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double theta,
                       double theta_t, int32_t leaf_size, double* energy, int64_t* stats);
 
+/* phi = K psi for the high-order (kind TPE_BCT_HIGH) or low-order (TPE_BCT_LOW)
+ * edge kernel of the Sobolev inner product by the block cluster tree: the
+ * stage-2 oracle's bct_matvec_kernel (oracle/tpe_stage2_oracle.py:649-703), same
+ * tree, same block recursion and admissibility (>= 3 edges in the block, no
+ * shared vertex, max radius / distance <= theta, max tangent radius <=
+ * theta_t; theta_t < 0 means 1.5 theta), node kernel bct_kernel_node (:634-643)
+ * and exact pair kernel exact_edge_kernel_pair (:706-730). psi and phi are E x
+ * ncols host arrays, ncols 1 or 3. theta = 0 gives the exact product. stats
+ * (nullable, 4): block-tree leaves, admissible blocks, direct blocks, direct
+ * pairs. */
+enum { TPE_BCT_HIGH = 0, TPE_BCT_LOW = 1 };
+int32_t tpe_bct_matvec(tpe_ctx* ctx, const double* xyz, int32_t kind, const double* psi,
+                       int32_t ncols, double epsilon, double theta, double theta_t,
+                       int32_t leaf_size, double* phi, int64_t* stats);
+
 /* Energies of `ncurves` curves that share this context's topology (e.g. the K
  * tau-trial candidates of one line search) in one launch: xyz is
  * ncurves x V x 3, energies[ncurves]. */

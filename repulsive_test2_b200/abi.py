@@ -43,6 +43,7 @@ PROJECTION_REASSEMBLE, PROJECTION_FROZEN = 0, 1
 FACTOR_LDLT, FACTOR_LU = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 GEMM_FP64, GEMM_INT8_EMULATED = 0, 1
+BCT_HIGH, BCT_LOW = 0, 1
 
 PHASE_KEYS = ["dE", "energy", "bHigh", "bLow", "assembleA", "expand", "saddle", "factor",
               "projection", "lineSearch", "step", "refine"]
@@ -154,6 +155,8 @@ SIGNATURES = {
     "tpe_penalty_energy": (C.c_int32, [vp, dp, C.POINTER(tpe_penalties), dp]),
     "tpe_penalty_gradient": (C.c_int32, [vp, dp, C.POINTER(tpe_penalties), dp]),
     "tpe_energy_batch": (C.c_int32, [vp, dp, C.c_int32, C.POINTER(tpe_params), C.c_int32, dp]),
+    "tpe_bct_matvec": (C.c_int32, [vp, dp, C.c_int32, dp, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                   C.c_int32, dp, C.POINTER(C.c_int64)]),
     "tpe_energy_bh": (C.c_int32, [vp, dp, C.POINTER(tpe_params), C.c_double, C.c_double, C.c_int32, dp,
                                   C.POINTER(C.c_int64)]),
     "tpe_sobolev_step_device": (C.c_int32, [vp, C.c_void_p, C.POINTER(tpe_constraint), C.c_int32,

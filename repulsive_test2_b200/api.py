@@ -189,6 +189,25 @@ def bhEnergy(vertices, edges, alpha=3.0, beta=6.0, epsilon=1e-10, theta=0.5, lea
     return out.value, {"visits": int(st[0]), "approximated_edge_refs": int(st[1]), "direct_pairs": int(st[2])}
 
 
+def bctMatvec(vertices, edges, psi, kind="high", epsilon=1e-10, theta=0.5, leafSize=8, thetaT=None):
+    """phi = K psi for the high- or low-order edge kernel by the block cluster tree, the
+    stage-2 oracle's bct_matvec_kernel (oracle/tpe_stage2_oracle.py:649-703): (phi, {"leaves",
+    "admissible_blocks", "direct_blocks", "direct_pairs"}). psi is E or E x 3."""
+    ctx = context()
+    v = _v(vertices)
+    ctx.topology(v, edges)
+    ps = np.ascontiguousarray(np.asarray(psi, dtype=np.float64))
+    ncols = 1 if ps.ndim == 1 else ps.shape[1]
+    phi = np.zeros_like(ps)
+    st = (C.c_int64 * 4)()
+    ctx.check(ctx.lib.tpe_bct_matvec(ctx.ptr, _dp(v), abi.BCT_HIGH if kind == "high" else abi.BCT_LOW,
+                                     _dp(ps), ncols, float(epsilon), float(theta),
+                                     -1.0 if thetaT is None else float(thetaT), int(leafSize), _dp(phi), st),
+              "bctMatvec")
+    return phi, {"leaves": int(st[0]), "admissible_blocks": int(st[1]), "direct_blocks": int(st[2]),
+                 "direct_pairs": int(st[3])}
+
+
 # ---- innerProduct.ts --------------------------------------------------------------
 
 def _assemble(vertices, edges, which, alpha, beta, epsilon):

@@ -1417,6 +1417,18 @@ int32_t tpe_energy_bh(tpe_ctx* ctx, const double* xyz, const tpe_params* p, doub
     });
 }
 
+int32_t tpe_bct_matvec(tpe_ctx* ctx, const double* xyz, int32_t kind, const double* psi,
+                       int32_t ncols, double epsilon, double theta, double theta_t,
+                       int32_t leaf_size, double* phi, int64_t* stats) {
+    return guarded(ctx, [&]() -> int32_t {
+        TPE_TRY(check_topology(ctx));
+        if (!xyz || !psi || !phi) return TPE_ERR_BAD_ARG;
+        TPE_TRY(upload(ctx, ctx->pos, xyz, sizeof(double) * 3 * (size_t)ctx->V));
+        return bct_matvec(ctx, xyz, ctx->pos.as<double>(), kind, psi, ncols, epsilon, theta,
+                          theta_t < 0.0 ? 1.5 * theta : theta_t, leaf_size, phi, stats);
+    });
+}
+
 int32_t tpe_energy_grad(tpe_ctx* ctx, const double* xyz, const tpe_params* p, double* energy,
                         double* grad) {
     return guarded(ctx, [&]() -> int32_t {

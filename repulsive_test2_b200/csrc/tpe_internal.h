@@ -255,6 +255,13 @@ int32_t bh_energy(tpe_ctx* ctx, const double* h_xyz, const double* d_xyz, double
                   double eps, double theta, double theta_t, int32_t leaf, double* energy,
                   int64_t* stats);
 
+// phi = K psi (E x nr, nr = 1 or 3; host arrays) for the high (kind 0) or low
+// (kind 1) edge kernel by the block cluster tree (bh.cu). stats (nullable, 4):
+// block-tree leaves, admissible blocks, direct blocks, direct pairs.
+int32_t bct_matvec(tpe_ctx* ctx, const double* h_xyz, const double* d_xyz, int32_t kind,
+                   const double* h_psi, int32_t nr, double eps, double theta, double theta_t,
+                   int32_t leaf, double* h_phi, int64_t* stats);
+
 // ---- mixed precision energy (pair_mixed.cu) ----------------------------------
 // FP32 pair terms, FP64 sums: tpe_energy_batch with TPE_PRECISION_MIXED only.
 int32_t edge_prep_mixed(tpe_ctx* ctx, const double* d_pos, int32_t ncurves, double eps,

@@ -1,5 +1,6 @@
-"""Regenerates tests/golden/bh_cases.npz: Barnes-Hut energies of the reference's
-own stage-2 oracle (oracle/tpe_stage2_oracle.py bh_energy) with its counts.
+"""Regenerates tests/golden/bh_cases.npz and bct_cases.npz: Barnes-Hut energies
+and block-cluster-tree kernel products of the reference's own stage-2 oracle
+(oracle/tpe_stage2_oracle.py bh_energy, bct_matvec_kernel) with their counts.
 
 Run where a checkout of the reference repository exists, naming its root in
 REFERENCE_ROOT (required; there is no default); the GPU tests only read the
@@ -15,7 +16,10 @@ at the default (0.5, 0.75, 8) and at (0.5, 0.75, 4); and a small loop network
 (3 loops of 64 joined at 2 junctions: vertices of degree 3, not one closed loop).
 Each case stores vertices, edges, (alpha, beta, epsilon, theta, theta_t, leaf),
 the energy, the exact energy (calculate_energy) and the counts (visits,
-approximated edge references, direct pairs).
+approximated edge references, direct pairs). The kernel-product cases (high and
+low kernels, theta = 0 on the 60-point trefoil, a three-column psi) store psi,
+phi, the dense product exact_edge_kernel_sym @ psi and the block counts
+(leaves, admissible blocks, direct blocks, direct pairs).
 """
 from __future__ import annotations
 
@@ -75,6 +79,39 @@ def main():
                                         dtype=np.int64)
         print(f"{name}: E={len(e)} bh={en:.17g} exact={ex:.17g} rel={abs(en - ex) / abs(ex):.2e} {st}")
     np.savez_compressed(os.path.join(HERE, "bh_cases.npz"), **out)
+
+    # block-cluster-tree kernel products (bct_matvec_kernel)
+    bct = {}
+    vec = np.stack([np.sin(np.arange(120) * 0.61) + 0.2, np.cos(np.arange(120) * 0.37),
+                    np.sin(np.arange(120) * 0.11) - 0.5], axis=1)
+    bcases = [
+        ("trefoil60_exact_leaf2_high", v60, e60, "high", 0.0, 0.0, 2, None),
+        ("trefoil60_exact_leaf8_low", v60, e60, "low", 0.0, 0.0, 8, None),
+        ("trefoil120_high", v120, e120, "high", 0.5, 0.75, 4, None),
+        ("trefoil120_low", v120, e120, "low", 0.5, 0.75, 4, None),
+        ("trefoil120_high_vec", v120, e120, "high", 0.5, 0.75, 4, vec),
+        ("walk512_high", vrw, erw, "high", 0.5, 0.75, 8, None),
+        ("walk512_low", vrw, erw, "low", 0.5, 0.75, 8, None),
+        ("network_low", vnet, enet, "low", 0.5, 0.75, 4, None),
+    ]
+    for name, v, e, kind, th, tht, leaf, psi in bcases:
+        v = np.asarray(v, dtype=np.float64)
+        e = np.asarray(e, dtype=np.int64)
+        if psi is None:
+            psi = np.sin(np.arange(len(e)) * 0.61) + 0.2
+        phi, st = O.bct_matvec_kernel(v, e, EPS, psi, kind, theta=th, leaf_size=leaf, theta_t=tht)
+        exact = O.exact_edge_kernel_sym(v, e, EPS, kind) @ psi
+        bct[name + "/vertices"] = v
+        bct[name + "/edges"] = e.astype(np.int32)
+        bct[name + "/params"] = np.array([EPS, th, tht, leaf, 0 if kind == "high" else 1], dtype=np.float64)
+        bct[name + "/psi"] = np.asarray(psi, dtype=np.float64)
+        bct[name + "/phi"] = phi
+        bct[name + "/exact"] = exact
+        bct[name + "/stats"] = np.array([st["leaves"], st["admissible_blocks"], st["direct_blocks"],
+                                         st["direct_pairs"]], dtype=np.int64)
+        rel = np.linalg.norm(phi - exact) / max(1.0, np.linalg.norm(exact))
+        print(f"{name}: E={len(e)} rel_vs_exact={rel:.2e} {st}")
+    np.savez_compressed(os.path.join(HERE, "bct_cases.npz"), **bct)
 
 
 if __name__ == "__main__":

@@ -1,5 +1,6 @@
-"""The Barnes-Hut energy (tpe_energy_bh), the hierarchical path of the
-reference's stage-2 oracle (oracle/tpe_stage2_oracle.py bh_energy).
+"""The hierarchical path of the reference's stage-2 oracle
+(oracle/tpe_stage2_oracle.py): the Barnes-Hut energy (tpe_energy_bh, bh_energy)
+and the block-cluster-tree kernel product (tpe_bct_matvec, bct_matvec_kernel).
 
 Against the oracle's own outputs (tests/golden/bh_cases.npz, written by
 tests/golden/make_bh.py from the reference's Python oracle): the energy within
@@ -65,3 +66,46 @@ def test_bh_gates_at_large_sizes():
     assert rel05 <= 5e-2 and rel025 <= rel05
     # the tree replaces most of the n^2 pairs
     assert st05["direct_pairs"] < 0.1 * n * n
+
+
+BCT_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bct_cases.npz")
+
+
+def _bct_names():
+    return sorted({k.split("/")[0] for k in np.load(BCT_GOLDEN).files})
+
+
+@pytest.mark.parametrize("name", _bct_names())
+def test_bct_matvec_matches_reference_oracle(name):
+    """tpe_bct_matvec against the oracle's bct_matvec_kernel: phi within 1e-12 of
+    its norm and the block counts exactly (same tree, same block recursion)."""
+    z = np.load(BCT_GOLDEN)
+    v, e, psi = z[name + "/vertices"], z[name + "/edges"], z[name + "/psi"]
+    eps, th, tht, leaf, kind = z[name + "/params"]
+    want, exact = z[name + "/phi"], z[name + "/exact"]
+    phi, st = T.bctMatvec(v, e, psi, "high" if kind == 0 else "low", epsilon=eps, theta=th,
+                          leafSize=int(leaf), thetaT=tht)
+    assert np.linalg.norm(phi - want) <= 1e-12 * np.linalg.norm(want)
+    assert [st["leaves"], st["admissible_blocks"], st["direct_blocks"], st["direct_pairs"]] == \
+        list(z[name + "/stats"])
+    if th == 0.0:
+        assert np.linalg.norm(phi - exact) <= 1e-12 * np.linalg.norm(exact)
+
+
+def test_bct_matvec_large_sizes():
+    """theta = 0 is the exact product and the error shrinks with theta, at 8192 edges."""
+    n = 8192
+    t = np.linspace(0.0, 2.0 * np.pi, n, endpoint=False)
+    v = np.stack([np.sin(t) + 2.0 * np.sin(2.0 * t), np.cos(t) - 2.0 * np.cos(2.0 * t), -np.sin(3.0 * t)],
+                 axis=1) * 0.25
+    e = np.asarray([[i, (i + 1) % n] for i in range(n)], dtype=np.int32)
+    psi = np.sin(np.arange(n) * 0.61) + 0.2
+    for kind in ("high", "low"):
+        ex, st0 = T.bctMatvec(v, e, psi, kind, theta=0.0, leafSize=8)
+        assert st0["admissible_blocks"] == 0 and st0["direct_pairs"] == n * (n - 3)
+        p05, st05 = T.bctMatvec(v, e, psi, kind, theta=0.5, leafSize=8, thetaT=0.75)
+        p025, _ = T.bctMatvec(v, e, psi, kind, theta=0.25, leafSize=8, thetaT=0.5)
+        r05 = np.linalg.norm(p05 - ex) / np.linalg.norm(ex)
+        r025 = np.linalg.norm(p025 - ex) / np.linalg.norm(ex)
+        assert st05["admissible_blocks"] > 0 and st05["direct_pairs"] < 0.2 * n * n
+        assert r025 <= r05
