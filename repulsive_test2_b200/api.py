@@ -208,6 +208,49 @@ def bctMatvec(vertices, edges, psi, kind="high", epsilon=1e-10, theta=0.5, leafS
                  "direct_pairs": int(st[3])}
 
 
+def bctApplyB(vertices, edges, u, kind="high", epsilon=1e-10, theta=0.5, leafSize=8, thetaT=None):
+    """The high-order (B) or low-order (B0) Sobolev operator applied to a vertex function u
+    through block-cluster-tree kernel products, the stage-2 oracle's bct_apply_B_scalar
+    (oracle/tpe_stage2_oracle.py:742-805): low: z = (K1 y - K y) for y the edge averages of u,
+    spread half to each endpoint; high: y = D u (edge differences along the unit tangents),
+    z = K1 y - K y, out = D^T z; K1 = K 1. theta = 0 gives B u (B0 u) of the dense assembly
+    (innerProduct.ts assembleBHighFlat / assembleBLowFlat). Returns (out, stats) with the two
+    products' counts prefixed K1_ and Ky_."""
+    v = _v(vertices)
+    e = np.asarray(edges, dtype=np.int64).reshape(-1, 2)
+    u = np.asarray(u, dtype=np.float64)
+    a, b = e[:, 0], e[:, 1]
+    ed = v[b] - v[a]
+    ell_raw = np.linalg.norm(ed, axis=1)
+    ell_eps = ell_raw + epsilon
+    T_ = np.zeros_like(ed)
+    mask = ell_raw >= 1e-14
+    T_[mask] = ed[mask] / ell_raw[mask, None]
+    ones = np.ones(len(e))
+    if kind == "low":
+        y = 0.5 * (u[a] + u[b])
+        K1, s1 = bctMatvec(v, e, ones, "low", epsilon, theta, leafSize, thetaT)
+        Ky, s2 = bctMatvec(v, e, y, "low", epsilon, theta, leafSize, thetaT)
+        z = K1 * y - Ky
+        out = np.zeros(len(v))
+        np.add.at(out, a, 0.5 * z)
+        np.add.at(out, b, 0.5 * z)
+    elif kind == "high":
+        y = ((u[b] - u[a]) / ell_eps)[:, None] * T_
+        K1, s1 = bctMatvec(v, e, ones, "high", epsilon, theta, leafSize, thetaT)
+        Ky, s2 = bctMatvec(v, e, y, "high", epsilon, theta, leafSize, thetaT)
+        z = K1[:, None] * y - Ky
+        coeff = np.einsum("ij,ij->i", z, T_) / ell_eps
+        out = np.zeros(len(v))
+        np.add.at(out, a, -coeff)
+        np.add.at(out, b, coeff)
+    else:
+        raise ValueError(kind)
+    stats = {"K1_" + k: x for k, x in s1.items()}
+    stats.update({"Ky_" + k: x for k, x in s2.items()})
+    return out, stats
+
+
 # ---- innerProduct.ts --------------------------------------------------------------
 
 def _assemble(vertices, edges, which, alpha, beta, epsilon):

@@ -111,6 +111,18 @@ def main():
                                          st["direct_pairs"]], dtype=np.int64)
         rel = np.linalg.norm(phi - exact) / max(1.0, np.linalg.norm(exact))
         print(f"{name}: E={len(e)} rel_vs_exact={rel:.2e} {st}")
+    # the Sobolev operators through the products (bct_apply_B_scalar)
+    u = np.sin(np.arange(120) * 0.7)
+    for kind in ("high", "low"):
+        name = f"applyB_trefoil120_{kind}"
+        o, st = O.bct_apply_B_scalar(v120, e120, EPS, u, kind, 0.5, 4, theta_t=0.75)
+        bct[name + "/vertices"] = v120
+        bct[name + "/edges"] = e120.astype(np.int32)
+        bct[name + "/params"] = np.array([EPS, 0.5, 0.75, 4, 0 if kind == "high" else 1], dtype=np.float64)
+        bct[name + "/u"] = u
+        bct[name + "/out"] = o
+        bct[name + "/stats"] = np.array([st[k] for k in sorted(st)], dtype=np.int64)
+        print(f"{name}: {st}")
     np.savez_compressed(os.path.join(HERE, "bct_cases.npz"), **bct)
 
 

@@ -71,8 +71,10 @@ def test_bh_gates_at_large_sizes():
 BCT_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bct_cases.npz")
 
 
-def _bct_names():
-    return sorted({k.split("/")[0] for k in np.load(BCT_GOLDEN).files})
+def _bct_names(prefix=""):
+    return sorted({k.split("/")[0] for k in np.load(BCT_GOLDEN).files if k.endswith("/params")
+                   and k.startswith(prefix) and not k.startswith("applyB")} if not prefix else
+                  {k.split("/")[0] for k in np.load(BCT_GOLDEN).files if k.startswith(prefix)})
 
 
 @pytest.mark.parametrize("name", _bct_names())
@@ -109,3 +111,30 @@ def test_bct_matvec_large_sizes():
         r025 = np.linalg.norm(p025 - ex) / np.linalg.norm(ex)
         assert st05["admissible_blocks"] > 0 and st05["direct_pairs"] < 0.2 * n * n
         assert r025 <= r05
+
+
+@pytest.mark.parametrize("name", _bct_names("applyB"))
+def test_bct_apply_B_matches_reference_oracle(name):
+    """The Sobolev operators through the products (bct_apply_B_scalar) at theta 0.5."""
+    z = np.load(BCT_GOLDEN)
+    v, e, u = z[name + "/vertices"], z[name + "/edges"], z[name + "/u"]
+    eps, th, tht, leaf, kind = z[name + "/params"]
+    out, st = T.bctApplyB(v, e, u, "high" if kind == 0 else "low", epsilon=eps, theta=th,
+                          leafSize=int(leaf), thetaT=tht)
+    want = z[name + "/out"]
+    # K1 y - K y cancels: the bound is on the size of the two products' difference
+    assert np.linalg.norm(out - want) <= 1e-11 * np.linalg.norm(want)
+    assert [st[k] for k in sorted(st)] == list(z[name + "/stats"])
+
+
+def test_bct_apply_B_theta0_is_the_dense_gram_product():
+    """theta = 0: B u and B0 u from the hierarchical products equal the products with the
+    dense matrices of the step's own assembly kernels (assembleBHighFlat / assembleBLowFlat)."""
+    v, e = F.random_walk_knot(512, seed=9)
+    u = np.sin(np.arange(512) * 0.7)
+    for kind, assemble in (("high", T.assembleBHighFlat), ("low", T.assembleBLowFlat)):
+        M = np.asarray(assemble(v, e)).reshape(512, 512)
+        out, st = T.bctApplyB(v, e, u, kind, theta=0.0, leafSize=8)
+        want = M @ u
+        assert st["Ky_admissible_blocks"] == 0
+        assert np.linalg.norm(out - want) <= 1e-12 * np.linalg.norm(M) * np.linalg.norm(u)
