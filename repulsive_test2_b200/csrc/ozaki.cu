@@ -448,9 +448,11 @@ int32_t ozaki_gemm_nt(tpe_ctx* ctx, const DGemmArgs& g, cudaStream_t stream, int
     }
     const int64_t kp = round_up(g.K, kBK);
     // B may be a band of A's rows (a symmetric update): its digits are then A's
-    const int64_t off = (g.B - g.A) / (g.lda > 0 ? g.lda : 1);
-    const bool shared = g.lda == g.ldb && g.B >= g.A && (g.B - g.A) % g.lda == 0 &&
-                        off + g.N <= g.M;
+    // (addresses compared as integers: A and B may be separate allocations)
+    const uintptr_t pa_ = (uintptr_t)g.A, pb_ = (uintptr_t)g.B;
+    const uintptr_t row = (uintptr_t)g.lda * sizeof(double);
+    const int64_t off = pb_ >= pa_ ? (int64_t)((pb_ - pa_) / row) : -1;
+    const bool shared = g.lda == g.ldb && pb_ >= pa_ && (pb_ - pa_) % row == 0 && off + g.N <= g.M;
     const int64_t mp = round_up(g.M, kBM);
     const int64_t np = shared ? 0 : round_up(g.N, kBN);
     const size_t need = ozaki_scratch_bytes(g.M, shared ? 0 : g.N, g.K);
