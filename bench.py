@@ -166,6 +166,24 @@ def extras(args):
                                                   np.linalg.norm(finals["fp64"]))
     net["speedup_vs_fp64"] = net["fp64"]["ms_per_step"] / net["mixed"]["ms_per_step"]
     out["network"] = net
+    # sizes that are not a multiple of 128 (the mixed factor pads to the next multiple)
+    rag = {"workload": "random-walk knot, [barycenter, totalLength], mixed, 8 step sizes per batch; one "
+                       "step from the initial curve, best of 3 after one warm-up (wall time, host API)"}
+    for Vr in (4096, 4097, 6000):
+        rv, re_ = F.random_walk_knot(Vr, seed=1)
+        rb = [T.barycenterBlock(T.barycenterTarget(rv, re_)), T.totalLengthBlock(T.totalLength(rv, re_))]
+        ro = {"projectionMode": "frozen", "precision": "mixed", "trials": 8,
+              "energyBefore": T.calculateEnergy(rv, re_)}
+        T.sobolevStepSet(rv, re_, None, rb, ro)
+        best = None
+        for _ in range(3):
+            t0 = time.perf_counter()
+            T.sobolevStepSet(rv, re_, None, rb, ro)
+            dt_ = time.perf_counter() - t0
+            best = dt_ if best is None else min(best, dt_)
+        rag[f"V{Vr}_ms"] = best * 1e3
+    rag["ratio_4097_over_4096"] = rag["V4097_ms"] / rag["V4096_ms"]
+    out["ragged_sizes"] = rag
     # Barnes-Hut energy (the hierarchical path) against the exact GPU energy on a
     # smooth curve far larger than the step's V
     bh = {"workload": "closed trefoil (the stage-2 oracle's check curve), theta 0.5, theta_t 0.75, leaf 8; "
