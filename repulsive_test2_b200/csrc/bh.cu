@@ -24,6 +24,8 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "tpe_internal.h"
@@ -73,12 +75,21 @@ struct Builder {
     const std::vector<double>& T;  // E x 3 unit tangents
     const std::vector<double>& m;  // E masses (ell_eps)
     int32_t leaf;
-    std::vector<int32_t> perm;
+    int32_t* perm;                 // shared; a builder writes only its own ranges
     std::vector<Node> nodes;
     std::vector<double> tmp;
+    std::vector<std::pair<double, int32_t>> keyed;
+    // subtrees at depth split_depth are left to other builders: (begin, count,
+    // parent node, is-left) each, the parent's child link holding -2 - task
+    int32_t split_depth = -1;
+    struct Task {
+        int32_t begin, count, parent;
+        bool left;
+    };
+    std::vector<Task> tasks;
 
-    int32_t rec(int32_t begin, int32_t count) {
-        const int32_t* idx = perm.data() + begin;
+    int32_t rec(int32_t begin, int32_t count, int32_t depth = 0) {
+        const int32_t* idx = perm + begin;
         tmp.resize((size_t)count);
         for (int32_t k = 0; k < count; k++) tmp[k] = m[idx[k]];
         const double msum = np_pairwise_sum(tmp.data(), (size_t)count);
@@ -128,15 +139,28 @@ struct Builder {
                 }
             const std::vector<double>& X = dim < 3 ? C : T;
             const int dd = dim % 3;
-            std::stable_sort(perm.begin() + begin, perm.begin() + begin + count,
-                             [&](int32_t a, int32_t b) { return X[3 * (size_t)a + dd] < X[3 * (size_t)b + dd]; });
+            keyed.resize((size_t)count);
+            for (int32_t k = 0; k < count; k++) keyed[k] = {X[3 * (size_t)idx[k] + dd], idx[k]};
+            std::stable_sort(keyed.begin(), keyed.end(),
+                             [](const std::pair<double, int32_t>& a, const std::pair<double, int32_t>& b) {
+                                 return a.first < b.first;
+                             });
+            for (int32_t k = 0; k < count; k++) perm[begin + k] = keyed[k].second;
             const int32_t mid = count / 2;
-            const int32_t l = rec(begin, mid);
-            const int32_t r = rec(begin + mid, count - mid);
+            int32_t l, r;
+            if (depth + 1 == split_depth) {
+                tasks.push_back({begin, mid, me, true});
+                l = -2 - (int32_t)(tasks.size() - 1);
+                tasks.push_back({begin + mid, count - mid, me, false});
+                r = -2 - (int32_t)(tasks.size() - 1);
+            } else {
+                l = rec(begin, mid, depth + 1);
+                r = rec(begin + mid, count - mid, depth + 1);
+                nodes[l].parent = me;
+                nodes[r].parent = me;
+            }
             nodes[me].left = l;
             nodes[me].right = r;
-            nodes[l].parent = me;
-            nodes[r].parent = me;
         }
         return me;
     }
@@ -284,13 +308,55 @@ void build_tree(const tpe_ctx* ctx, const double* h_xyz, double eps, int32_t lea
         for (int d = 0; d < 3; d++) tr.T[3 * (size_t)I + d] = ell >= kTangentTol ? e[d] / ell : 0.0;
         tr.m[I] = ell + eps;
     }
-    Builder B{tr.C, tr.T, tr.m, leaf, {}, {}, {}};
-    B.perm.resize((size_t)E);
-    std::iota(B.perm.begin(), B.perm.end(), 0);
-    B.nodes.reserve(2 * (size_t)E / std::max(1, leaf) + 2);
-    B.rec(0, E);
-    tr.nodes.swap(B.nodes);
-    tr.perm.swap(B.perm);
+    tr.perm.resize((size_t)E);
+    std::iota(tr.perm.begin(), tr.perm.end(), 0);
+    // The top levels on this thread; below them, subtrees on their own threads
+    // (disjoint ranges of the permutation, the same arithmetic), then joined.
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    int32_t split = 0;
+    while ((1u << split) < std::min(hw, 16u) && ((int64_t)E >> split) > 4 * (int64_t)leaf + 4096) split++;
+    Builder top{tr.C, tr.T, tr.m, leaf, tr.perm.data(), {}, {}, {}, split > 0 ? split : -1, {}};
+    top.rec(0, E);
+    std::vector<Builder> sub;
+    sub.reserve(top.tasks.size());
+    for (size_t i = 0; i < top.tasks.size(); i++)
+        sub.push_back(Builder{tr.C, tr.T, tr.m, leaf, tr.perm.data(), {}, {}, {}, -1, {}});
+    {
+        // a failure inside a worker (allocation) is carried back to this thread
+        std::vector<char> failed(top.tasks.size(), 0);
+        std::vector<std::thread> th;
+        try {
+            for (size_t i = 0; i < top.tasks.size(); i++)
+                th.emplace_back([&, i] {
+                    try {
+                        sub[i].rec(top.tasks[i].begin, top.tasks[i].count);
+                    } catch (...) {
+                        failed[i] = 1;
+                    }
+                });
+        } catch (...) {
+            for (auto& x : th) x.join();
+            throw;
+        }
+        for (auto& x : th) x.join();
+        for (char f : failed)
+            if (f) throw std::bad_alloc();
+    }
+    tr.nodes.swap(top.nodes);
+    for (size_t i = 0; i < sub.size(); i++) {
+        const int32_t base = (int32_t)tr.nodes.size();
+        for (Node nd : sub[i].nodes) {
+            if (nd.left >= 0) {
+                nd.left += base;
+                nd.right += base;
+            }
+            if (nd.parent >= 0) nd.parent += base;
+            tr.nodes.push_back(nd);
+        }
+        const Builder::Task& tk = top.tasks[i];
+        tr.nodes[base].parent = tk.parent;
+        (tk.left ? tr.nodes[tk.parent].left : tr.nodes[tk.parent].right) = base;
+    }
     tr.where.assign((size_t)E, 0);
     for (int32_t k = 0; k < E; k++) tr.where[tr.perm[k]] = k;
 }
