@@ -132,14 +132,29 @@ def extras(args):
         b.step(xs, sets, ob)
     dtb = (time.perf_counter() - t0) / nb
     t0 = time.perf_counter()
+    per_curve = []
     for (cv, ce), st_ in zip(curves, sets):
+        t1 = time.perf_counter()
         T.sobolevStepSet(cv, ce, None, st_, ob)
+        per_curve.append((len(cv), time.perf_counter() - t1))
     dts = time.perf_counter() - t0
+    # the sequential steps' time by size octave: where the batch's time goes
+    octaves = {}
+    for nv_, dtc in per_curve:
+        lo_ = 256
+        while lo_ * 2 <= nv_ and lo_ < 2048:
+            lo_ *= 2
+        key = f"V{lo_}-{2 * lo_}"
+        octaves.setdefault(key, [0, 0.0])
+        octaves[key][0] += 1
+        octaves[key][1] += dtc * 1e3
     b.close()
     out["batch"] = {"workload": "64 curves, V log-uniform in [256, 4096] (trefoil / torus knots / random "
                                 "walks), [barycenter, totalLength], mixed, 8 step sizes per projection batch",
                     "curve_steps_per_s": 64 / dtb, "ms_per_batch_step": dtb * 1e3,
-                    "sequential_curve_steps_per_s": 64 / dts}
+                    "sequential_curve_steps_per_s": 64 / dts,
+                    "sequential_ms_by_octave": {k: {"curves": c, "ms": round(t_, 2)}
+                                                for k, (c, t_) in sorted(octaves.items())}}
     # loop network
     PEN = {"totalLength": 1.0, "lengthDiff": 10.0, "field": {"weight": 5.0, "X": [0.5, 1.0, 0.0]}}
     nv, ne = F.loop_network(loops=12, n=1024, junctions=8, seed=5)
