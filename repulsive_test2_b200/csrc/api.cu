@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "tpe_internal.h"
+#include <cstring>
 
 namespace tpe {
 
@@ -61,6 +62,35 @@ KernelScope::KernelScope(tpe_ctx* c, int g, int64_t n) : ctx(c), group(g) {
 
 KernelScope::~KernelScope() {
     if (b) cudaEventRecord(b, ctx->stream);
+}
+
+int32_t download_many(tpe_ctx* ctx, cudaStream_t stream, const HostCopy* copies, int n) {
+    size_t total = 0;
+    for (int i = 0; i < n; i++) total += (copies[i].bytes + 15) / 16 * 16;
+    if (total > ctx->h_stage_bytes) {
+        TPE_CUDA_TRY(cudaStreamSynchronize(stream));
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr;
+        ctx->h_stage_bytes = 0;
+        const size_t want = std::max<size_t>(total + total / 4, 64 * 1024);
+        TPE_CUDA_TRY(cudaMallocHost(&ctx->h_stage, want));
+        ctx->h_stage_bytes = want;
+    }
+    unsigned char* stage = static_cast<unsigned char*>(ctx->h_stage);
+    size_t off = 0;
+    for (int i = 0; i < n; i++) {
+        if (copies[i].bytes)
+            TPE_CUDA_TRY(cudaMemcpyAsync(stage + off, copies[i].dev, copies[i].bytes,
+                                         cudaMemcpyDeviceToHost, stream));
+        off += (copies[i].bytes + 15) / 16 * 16;
+    }
+    TPE_CUDA_TRY(cudaStreamSynchronize(stream));
+    off = 0;
+    for (int i = 0; i < n; i++) {
+        if (copies[i].bytes) memcpy(copies[i].host, stage + off, copies[i].bytes);
+        off += (copies[i].bytes + 15) / 16 * 16;
+    }
+    return TPE_OK;
 }
 
 int32_t ensure(tpe_ctx* ctx, DevBuf& b, size_t bytes) {
@@ -116,9 +146,7 @@ int32_t upload(tpe_ctx* ctx, DevBuf& b, const void* host, size_t bytes) {
 }
 
 int32_t download(tpe_ctx* ctx, void* host, const void* dev, size_t bytes) {
-    TPE_CUDA_TRY(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return TPE_OK;
+    return download_on(ctx, ctx->stream, host, dev, bytes);
 }
 
 bool all_finite(const double* a, size_t n) {
@@ -952,14 +980,12 @@ int32_t project_batch_dev(tpe_ctx* ctx, const double* d_start, int32_t ntrial, c
         TPE_CUDA_TRY(cudaMemcpyAsync(d_idx, active.data(), sizeof(int32_t) * na,
                                      cudaMemcpyHostToDevice, ctx->stream));
         TPE_TRY(eval_constraints_batch(ctx, d_cur, m, d_idx, na, nb, k, d_phi, d_ns));
-        if (k > 0)
-            TPE_CUDA_TRY(cudaMemcpyAsync(phi.data(), d_phi, sizeof(double) * na * k,
-                                         cudaMemcpyDeviceToHost, ctx->stream));
-        TPE_CUDA_TRY(cudaMemcpyAsync(ns.data(), d_ns, sizeof(double) * na * 2 * nb,
-                                     cudaMemcpyDeviceToHost, ctx->stream));
-        TPE_CUDA_TRY(cudaMemcpyAsync(hbad.data(), d_bad, sizeof(int32_t) * ntrial,
-                                     cudaMemcpyDeviceToHost, ctx->stream));
-        TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        {
+            const HostCopy cp[3] = {{phi.data(), d_phi, k > 0 ? sizeof(double) * na * k : 0},
+                                    {ns.data(), d_ns, sizeof(double) * na * 2 * nb},
+                                    {hbad.data(), d_bad, sizeof(int32_t) * ntrial}};
+            TPE_TRY(download_many(ctx, ctx->stream, cp, 3));
+        }
         std::vector<int32_t> next;
         upd.clear();
         coef.clear();
@@ -1320,6 +1346,7 @@ void tpe_destroy(tpe_ctx* ctx) {
     }
     for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->fac_events) cudaEventDestroy(e);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->ev_prep) cudaEventDestroy(ctx->ev_prep);
     if (ctx->ev_grad) cudaEventDestroy(ctx->ev_grad);
     if (ctx->stream5) cudaStreamDestroy(ctx->stream5);

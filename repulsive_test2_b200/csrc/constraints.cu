@@ -440,13 +440,9 @@ int32_t eval_constraints(tpe_ctx* ctx, const double* d_pos, int32_t nblocks, int
             V, ctx->con_blocks.as<DevBlock>(), nblocks, d_C);
         TPE_CUDA_TRY(cudaGetLastError());
     }
-    if (k > 0)
-        TPE_CUDA_TRY(cudaMemcpyAsync(phi.data(), dphi, sizeof(double) * k, cudaMemcpyDeviceToHost,
-                                     ctx->stream));
-    TPE_CUDA_TRY(cudaMemcpyAsync(ns.data(), dns, sizeof(double) * 2 * nblocks,
-                                 cudaMemcpyDeviceToHost, ctx->stream));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return TPE_OK;
+    const HostCopy cp[2] = {{phi.data(), dphi, k > 0 ? sizeof(double) * k : 0},
+                            {ns.data(), dns, sizeof(double) * 2 * nblocks}};
+    return download_many(ctx, ctx->stream, cp, 2);
 }
 
 static PenW resolve(const tpe_penalties* p, bool* active) {

@@ -937,9 +937,7 @@ static int32_t reduce_to_host(tpe_ctx* ctx, double* part, int32_t nparts, double
     KernelScope ks(ctx, TPE_KGROUP_OTHER, 1);
     sum_kernel<<<1, 256, 0, ctx->stream>>>(part, nparts, dst);
     TPE_CUDA_TRY(cudaGetLastError());
-    TPE_CUDA_TRY(cudaMemcpyAsync(out, dst, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    TPE_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return TPE_OK;
+    return download_on(ctx, ctx->stream, out, dst, sizeof(double));
 }
 
 int32_t dot(tpe_ctx* ctx, int64_t n, const double* x, const double* y, double* out) {

@@ -1470,8 +1470,7 @@ int32_t mixed_solve(tpe_ctx* ctx, const double* d_A, const double* d_B, double* 
                 TPE_CUDA_TRY(cudaGetLastError());
             }
             TPE_TRY(dots(R, R, di, res2));
-            TPE_CUDA_TRY(cudaMemcpyAsync(hres.data(), res2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-            TPE_CUDA_TRY(cudaStreamSynchronize(st));
+            TPE_TRY(download_on(ctx, st, hres.data(), res2, sizeof(double) * n));
             done = true;
             for (int c = 0; c < n; c++)
                 if (!(hres[c] <= tol * tol * hbn[c])) done = false;

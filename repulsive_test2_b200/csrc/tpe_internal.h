@@ -170,6 +170,8 @@ struct tpe_ctx {
     tpe::DevBuf mx_d, mx_dinv, mx_S, mx_Lhi, mx_Llo, mx_Zhi, mx_Zlo, mx_Whi, mx_Wlo, mx_Thi, mx_Tlo,
         mx_vec, mx_part, mx_Zd, mx_Wd;
     tpe::MixedFactor mf;
+    void* h_stage = nullptr;  // pinned staging of small device-to-host copies (download_many)
+    size_t h_stage_bytes = 0;
     std::vector<double> h_tmp;
 
     // instrumentation: kernel launch count and per-group CUDA-event timing
@@ -228,6 +230,22 @@ int32_t guarded(tpe_ctx* ctx, F&& body) noexcept {
     return code;
 }
 int32_t ensure(tpe_ctx* ctx, DevBuf& b, size_t bytes);
+
+// Device-to-host copies through the context's pinned staging area: the copies
+// are issued on `stream`, the stream is synchronized once, and the bytes are
+// copied out on the host. Pageable copies from many host threads (the
+// multi-curve batch) would queue in the driver's shared staging buffer.
+struct HostCopy {
+    void* host;
+    const void* dev;
+    size_t bytes;
+};
+int32_t download_many(tpe_ctx* ctx, cudaStream_t stream, const HostCopy* copies, int n);
+inline int32_t download_on(tpe_ctx* ctx, cudaStream_t stream, void* host, const void* dev,
+                           size_t bytes) {
+    const HostCopy c{host, dev, bytes};
+    return download_many(ctx, stream, &c, 1);
+}
 
 // ---- pair kernels (pair_kernels.cu) ----------------------------------------
 // Per-edge records from interleaved positions: a = (p1, ell^eps), b = (p2, |e|).
