@@ -1,0 +1,67 @@
+"""Host logic of the hierarchical path, on the CPU: api.bctApplyB's glue around
+the block-cluster-tree products (the edge averages or tangential differences of
+u, K1 y - K y, the spread back to the vertices, after the stage-2 oracle's
+bct_apply_B_scalar, oracle/tpe_stage2_oracle.py:742-805). The two products are
+replaced by a dense numpy restatement of the exact edge kernels
+(exact_edge_kernel_pair, :712-740), which is what the device products return at
+theta = 0; the result must then be B u and B0 u of the C oracle's assembly
+(innerProduct.ts assembleBHighFlat / assembleBLowFlat)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from repulsive_test2_b200 import api as T
+from repulsive_test2_b200 import fixtures as F
+
+EPS = 1e-10
+
+
+def _dense_kernel(v, e, kind):
+    """K[I][J] for disjoint edges I != J (0 otherwise)."""
+    p = 7.0 / 3.0
+    E = len(e)
+    a, b = e[:, 0], e[:, 1]
+    d = v[b] - v[a]
+    lr = np.linalg.norm(d, axis=1)
+    ell = lr + EPS
+    Tn = np.where(lr[:, None] >= 1e-14, d / np.where(lr[:, None] > 0, lr[:, None], 1.0), 0.0)
+    K = np.zeros((E, E))
+    for I in range(E):
+        for J in range(E):
+            if I == J or len({a[I], b[I]} & {a[J], b[J]}):
+                continue
+            s1 = s2 = 0.0
+            for vi in (a[I], b[I]):
+                for vj in (a[J], b[J]):
+                    q = v[vi] - v[vj]
+                    dn = np.linalg.norm(q) + EPS
+                    if kind == "high":
+                        s1 += 1.0 / dn ** p
+                    else:
+                        s1 += (np.linalg.norm(np.cross(Tn[I], q)) + EPS) ** 2 / dn ** (4 + p)
+                        s2 += (np.linalg.norm(np.cross(Tn[J], -q)) + EPS) ** 2 / dn ** (4 + p)
+            K[I, J] = 2 * 0.25 * ell[I] * ell[J] * s1 if kind == "high" else 0.25 * ell[I] * ell[J] * (s1 + s2)
+    return K
+
+
+@pytest.mark.parametrize("kind", ["high", "low"])
+def test_apply_B_glue_against_dense_assembly(kind, monkeypatch):
+    v, e = F.random_walk_knot(48, seed=21)
+    e = np.asarray(e)
+    K = _dense_kernel(v, e, kind)
+
+    def fake_bct(vertices, edges, psi, kind_, epsilon=1e-10, theta=0.5, leafSize=8, thetaT=None):
+        assert kind_ == kind
+        stats = {"leaves": 1, "admissible_blocks": 0, "direct_blocks": 1, "direct_pairs": 0}
+        return K @ np.asarray(psi), stats
+
+    monkeypatch.setattr(T, "bctMatvec", fake_bct)
+    u = np.sin(np.arange(len(v)) * 0.7)
+    out, st = T.bctApplyB(v, e, u, kind, theta=0.0)
+    M = np.asarray(O.assemble(v, e, "B" if kind == "high" else "B0")).reshape(len(v), len(v))
+    want = M @ u
+    assert np.linalg.norm(out - want) <= 1e-12 * np.linalg.norm(M) * np.linalg.norm(u)
+    assert set(st) == {f"{p}_{k}" for p in ("K1", "Ky") for k in
+                       ("leaves", "admissible_blocks", "direct_blocks", "direct_pairs")}
