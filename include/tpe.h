@@ -275,6 +275,15 @@ int32_t tpe_energy_bh(tpe_ctx* ctx, const double* xyz, const tpe_params* p, doub
  * (nullable, 4): block-tree leaves, admissible blocks, direct blocks, direct
  * pairs. */
 enum { TPE_BCT_HIGH = 0, TPE_BCT_LOW = 1 };
+/* The edge tree those two calls build (build_edge_bvh, oracle/tpe_stage2_oracle.py:467-502),
+ * on the host only (no device, no context), for checking it node by node: per node
+ * node_f[9] = center xyz, mean tangent xyz, mass, rx, rT and node_i[4] = first
+ * position in perm, edge count, left, right (-1 for a leaf); perm[E] lists the
+ * edges so that every node's edges are one contiguous range. *n_nodes receives
+ * the node count; TPE_ERR_TOO_LARGE when it exceeds max_nodes. */
+int32_t tpe_edge_tree(const double* xyz, int32_t V, const int32_t* edges, int32_t E,
+                      double epsilon, int32_t leaf_size, int32_t max_nodes, double* node_f,
+                      int32_t* node_i, int32_t* perm, int32_t* n_nodes);
 int32_t tpe_bct_matvec(tpe_ctx* ctx, const double* xyz, int32_t kind, const double* psi,
                        int32_t ncols, double epsilon, double theta, double theta_t,
                        int32_t leaf_size, double* phi, int64_t* stats);

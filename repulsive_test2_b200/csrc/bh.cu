@@ -292,13 +292,13 @@ struct Tree {
     std::vector<int32_t> perm, where;  // edge at each position, position of each edge
 };
 
-void build_tree(const tpe_ctx* ctx, const double* h_xyz, double eps, int32_t leaf, Tree& tr) {
-    const int32_t E = ctx->E;
+void build_tree(const int32_t* edges, int32_t E, const double* h_xyz, double eps, int32_t leaf,
+                Tree& tr) {
     tr.C.assign((size_t)3 * E, 0.0);
     tr.T.assign((size_t)3 * E, 0.0);
     tr.m.assign((size_t)E, 0.0);
     for (int32_t I = 0; I < E; I++) {
-        const int32_t a = ctx->h_edges[2 * (size_t)I], b = ctx->h_edges[2 * (size_t)I + 1];
+        const int32_t a = edges[2 * (size_t)I], b = edges[2 * (size_t)I + 1];
         double e[3];
         for (int d = 0; d < 3; d++) {
             e[d] = h_xyz[3 * (size_t)b + d] - h_xyz[3 * (size_t)a + d];
@@ -377,7 +377,7 @@ int32_t bh_energy(tpe_ctx* ctx, const double* h_xyz, const double* d_xyz, double
         return TPE_OK;
     }
     Tree tr;
-    build_tree(ctx, h_xyz, eps, leaf, tr);
+    build_tree(ctx->h_edges.data(), ctx->E, h_xyz, eps, leaf, tr);
     const size_t nn = tr.nodes.size();
     const size_t bytes_nodes = sizeof(Node) * nn, bytes_idx = sizeof(int32_t) * (size_t)E;
     const size_t off_perm = (bytes_nodes + 255) / 256 * 256;
@@ -648,7 +648,7 @@ int32_t bct_matvec(tpe_ctx* ctx, const double* h_xyz, const double* d_xyz, int32
         return TPE_OK;
     }
     Tree tr;
-    build_tree(ctx, h_xyz, eps, leaf, tr);
+    build_tree(ctx->h_edges.data(), ctx->E, h_xyz, eps, leaf, tr);
     BctLists L;
     BctRec R{tr, ctx, kind, eps, theta, theta_t, L};
     R.rec(0, 0);
@@ -732,3 +732,37 @@ int32_t bct_matvec(tpe_ctx* ctx, const double* h_xyz, const double* d_xyz, int32
 }
 
 }  // namespace tpe
+
+// The edge tree alone, on the host (no device, no context): for checking the
+// builder against the stage-2 oracle's build_edge_bvh node by node.
+extern "C" int32_t tpe_edge_tree(const double* xyz, int32_t V, const int32_t* edges, int32_t E,
+                                 double epsilon, int32_t leaf_size, int32_t max_nodes,
+                                 double* node_f, int32_t* node_i, int32_t* perm,
+                                 int32_t* n_nodes) {
+    try {
+        if (!xyz || !edges || !node_f || !node_i || !perm || !n_nodes || V < 0 || E < 1 ||
+            leaf_size < 1)
+            return TPE_ERR_BAD_ARG;
+        for (int64_t q = 0; q < 2 * (int64_t)E; q++)
+            if (edges[q] < 0 || edges[q] >= V) return TPE_ERR_BAD_ARG;
+        tpe::Tree tr;
+        tpe::build_tree(edges, E, xyz, epsilon, leaf_size, tr);
+        *n_nodes = (int32_t)tr.nodes.size();
+        if ((int64_t)tr.nodes.size() > max_nodes) return TPE_ERR_TOO_LARGE;
+        for (size_t i = 0; i < tr.nodes.size(); i++) {
+            const tpe::Node& nd = tr.nodes[i];
+            const double f[9] = {nd.cx, nd.cy, nd.cz, nd.tx, nd.ty, nd.tz, nd.mass, nd.rx, nd.rT};
+            for (int q = 0; q < 9; q++) node_f[9 * i + q] = f[q];
+            node_i[4 * i] = nd.begin;
+            node_i[4 * i + 1] = nd.count;
+            node_i[4 * i + 2] = nd.left;
+            node_i[4 * i + 3] = nd.right;
+        }
+        for (int32_t k = 0; k < E; k++) perm[k] = tr.perm[k];
+        return TPE_OK;
+    } catch (const std::bad_alloc&) {
+        return TPE_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        return TPE_ERR_INTERNAL;
+    }
+}

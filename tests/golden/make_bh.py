@@ -19,7 +19,9 @@ the energy, the exact energy (calculate_energy) and the counts (visits,
 approximated edge references, direct pairs). The kernel-product cases (high and
 low kernels, theta = 0 on the 60-point trefoil, a three-column psi) store psi,
 phi, the dense product exact_edge_kernel_sym @ psi and the block counts
-(leaves, admissible blocks, direct blocks, direct pairs).
+(leaves, admissible blocks, direct blocks, direct pairs). bh_trees.npz holds the
+oracle's trees (build_edge_bvh) node by node: center, mean tangent, mass, radii,
+children and edge lists, for a trefoil, the loop network and a 20000-edge walk.
 """
 from __future__ import annotations
 
@@ -111,6 +113,26 @@ def main():
                                          st["direct_pairs"]], dtype=np.int64)
         rel = np.linalg.norm(phi - exact) / max(1.0, np.linalg.norm(exact))
         print(f"{name}: E={len(e)} rel_vs_exact={rel:.2e} {st}")
+    # the oracle's trees themselves (build_edge_bvh), node by node in its preorder
+    trees = {}
+    vbig, ebig = fixtures.random_walk_knot(20000, seed=13)
+    for name, v, e, leaf in (("trefoil120_leaf4", v120, e120, 4), ("network_leaf4", vnet, enet, 4),
+                             ("walk20000_leaf8", vbig, ebig, 8)):
+        v = np.asarray(v, dtype=np.float64)
+        e = np.asarray(e, dtype=np.int64)
+        nodes, _, _, _ = O.build_edge_bvh(v, e, EPS, leaf)
+        trees[name + "/vertices"] = v
+        trees[name + "/edges"] = e.astype(np.int32)
+        trees[name + "/leaf"] = np.array([leaf])
+        trees[name + "/f"] = np.array([np.concatenate([nd.center, nd.tangent, [nd.mass, nd.rx, nd.rT]])
+                                       for nd in nodes])
+        trees[name + "/links"] = np.array([[-1 if nd.left is None else nd.left,
+                                            -1 if nd.right is None else nd.right] for nd in nodes], dtype=np.int32)
+        trees[name + "/idx_off"] = np.cumsum([0] + [len(nd.indices) for nd in nodes]).astype(np.int64)
+        trees[name + "/idx"] = np.concatenate([nd.indices for nd in nodes]).astype(np.int32)
+        print(f"tree {name}: {len(nodes)} nodes")
+    np.savez_compressed(os.path.join(HERE, "bh_trees.npz"), **trees)
+
     # the Sobolev operators through the products (bct_apply_B_scalar)
     u = np.sin(np.arange(120) * 0.7)
     for kind in ("high", "low"):

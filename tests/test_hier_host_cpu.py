@@ -65,3 +65,53 @@ def test_apply_B_glue_against_dense_assembly(kind, monkeypatch):
     assert np.linalg.norm(out - want) <= 1e-12 * np.linalg.norm(M) * np.linalg.norm(u)
     assert set(st) == {f"{p}_{k}" for p in ("K1", "Ky") for k in
                        ("leaves", "admissible_blocks", "direct_blocks", "direct_pairs")}
+
+
+TREES = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                   "golden", "bh_trees.npz")
+
+
+@pytest.mark.parametrize("name", ["trefoil120_leaf4", "network_leaf4", "walk20000_leaf8"])
+def test_edge_tree_is_the_oracle_tree(name):
+    """tpe_edge_tree (the host builder the device traversals use, threaded below its top
+    levels for the 20000-edge walk) against the oracle's build_edge_bvh: the same nodes with
+    the same edges (in the same order in every leaf), and bit-equal centers, mean tangents,
+    masses and radii (the numpy summation orders are reproduced)."""
+    import ctypes as C
+
+    from repulsive_test2_b200 import abi
+
+    z = np.load(TREES)
+    v = np.ascontiguousarray(z[name + "/vertices"])
+    e = np.ascontiguousarray(z[name + "/edges"], dtype=np.int32)
+    leaf = int(z[name + "/leaf"][0])
+    f_o, links, off, idx = z[name + "/f"], z[name + "/links"], z[name + "/idx_off"], z[name + "/idx"]
+    E = len(e)
+    maxn = 4 * E + 8
+    node_f = np.zeros((maxn, 9))
+    node_i = np.zeros((maxn, 4), dtype=np.int32)
+    perm = np.zeros(E, dtype=np.int32)
+    nn = C.c_int32(0)
+    lib = abi.load_library()
+    rc = lib.tpe_edge_tree(v.ctypes.data_as(abi.dp), len(v), e.ctypes.data_as(abi.ip), E, EPS, leaf, maxn,
+                           node_f.ctypes.data_as(abi.dp), node_i.ctypes.data_as(abi.ip),
+                           perm.ctypes.data_as(abi.ip), C.byref(nn))
+    assert rc == 0
+    assert nn.value == len(f_o)
+    stack = [(0, 0)]
+    seen = 0
+    while stack:
+        mine, theirs = stack.pop()
+        seen += 1
+        b, cnt, l, r = node_i[mine]
+        want = idx[off[theirs]:off[theirs + 1]]
+        if l < 0:  # a leaf keeps its edges in the oracle's order
+            np.testing.assert_array_equal(perm[b:b + cnt], want)
+        else:  # an inner node's range is reordered by its children
+            np.testing.assert_array_equal(np.sort(perm[b:b + cnt]), np.sort(want))
+        np.testing.assert_array_equal(node_f[mine], f_o[theirs])
+        assert (l < 0) == (links[theirs][0] < 0)
+        if l >= 0:
+            stack.append((l, links[theirs][0]))
+            stack.append((r, links[theirs][1]))
+    assert seen == len(f_o)
