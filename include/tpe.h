@@ -104,7 +104,10 @@ typedef struct {
     double c1, shrink, tau0, tau_min;          /* 1e-4, 0.5, 1, 1e-12 */
     double proj_tol_abs, proj_tol_rel;         /* 1e-4, 1e-4 */
     int32_t proj_max_iter;                     /* 8 */
-    int32_t precision;             /* TPE_PRECISION_* (extension) */
+    int32_t precision;             /* TPE_PRECISION_* (extension): MIXED factors in 3xTF32 on the
+                                      tensor cores with an FP64 CG, or, for more than 64
+                                      constraint rows with frozen projection, forms the
+                                      explicit inverses from int8 digit products */
     int32_t trials;                /* frozen projection: step sizes projected together per batch
                                       (extension; default 8, 1 = one at a time; the accepted tau
                                       and vertices do not depend on it) */
@@ -128,8 +131,10 @@ typedef struct {
     int32_t projection_iterations; /* -1 = null */
     int32_t reason;                /* TPE_REASON_* */
     int32_t refine_iterations;     /* mixed path: CG iterations of the gradient solve;
-                                      0 = FP64 factorization, -1 = mixed requested but the
-                                      FP32 factor broke down or CG missed refine_tol (FP64 used) */
+                                      0 = FP64 factorization, or (large constraint sets)
+                                      the int8-tensor-core inverses; -1 = mixed requested but
+                                      the FP32 factor broke down, CG missed refine_tol, or the
+                                      int8 inverses missed the residual gate (FP64 used) */
     int32_t trials_evaluated;      /* tau trials whose energy was evaluated */
 } tpe_step_stats;
 
