@@ -70,6 +70,52 @@ double np_pairwise_sum(const double* a, size_t n) {
 
 inline double norm3(double x, double y, double z) { return std::sqrt((x * x + y * y) + z * z); }
 
+using Keyed = std::vector<std::pair<double, int32_t>>;
+
+// std::stable_sort on the key, with the range cut into up to `threads` pieces
+// sorted on their own threads and merged pairwise (std::merge takes from the
+// first range on ties, so the order is the same stable order).
+void stable_sort_keys(Keyed& a, int threads) {
+    auto less = [](const std::pair<double, int32_t>& x, const std::pair<double, int32_t>& y) {
+        return x.first < y.first;
+    };
+    const size_t n = a.size();
+    int p = 1;
+    while (p * 2 <= threads && n / (size_t)(p * 2) >= 16384) p *= 2;
+    if (p == 1) {
+        std::stable_sort(a.begin(), a.end(), less);
+        return;
+    }
+    std::vector<size_t> cut((size_t)p + 1);
+    for (int i = 0; i <= p; i++) cut[i] = n * (size_t)i / (size_t)p;
+    auto run = [&](std::vector<std::thread>& th, auto&& body, int count) {
+        try {
+            for (int i = 0; i < count; i++) th.emplace_back(body, i);
+        } catch (...) {
+            for (auto& t : th) t.join();
+            throw;
+        }
+        for (auto& t : th) t.join();
+    };
+    {
+        std::vector<std::thread> th;
+        run(th, [&](int i) { std::stable_sort(a.begin() + cut[i], a.begin() + cut[i + 1], less); }, p);
+    }
+    Keyed b(n);
+    for (int w = 1; w < p; w *= 2) {
+        std::vector<std::thread> th;
+        const int pairs = p / (2 * w);
+        run(th,
+            [&](int j) {
+                const size_t lo = cut[2 * w * j], mid = cut[2 * w * j + w], hi = cut[2 * w * (j + 1)];
+                std::merge(a.begin() + lo, a.begin() + mid, a.begin() + mid, a.begin() + hi,
+                           b.begin() + lo, less);
+            },
+            pairs);
+        a.swap(b);
+    }
+}
+
 struct Builder {
     const std::vector<double>& C;  // E x 3 midpoints
     const std::vector<double>& T;  // E x 3 unit tangents
@@ -78,7 +124,8 @@ struct Builder {
     int32_t* perm;                 // shared; a builder writes only its own ranges
     std::vector<Node> nodes;
     std::vector<double> tmp;
-    std::vector<std::pair<double, int32_t>> keyed;
+    Keyed keyed;
+    int sort_threads = 1;  // threads for the sort of one node (the top levels)
     // subtrees at depth split_depth are left to other builders: (begin, count,
     // parent node, is-left) each, the parent's child link holding -2 - task
     int32_t split_depth = -1;
@@ -141,10 +188,7 @@ struct Builder {
             const int dd = dim % 3;
             keyed.resize((size_t)count);
             for (int32_t k = 0; k < count; k++) keyed[k] = {X[3 * (size_t)idx[k] + dd], idx[k]};
-            std::stable_sort(keyed.begin(), keyed.end(),
-                             [](const std::pair<double, int32_t>& a, const std::pair<double, int32_t>& b) {
-                                 return a.first < b.first;
-                             });
+            stable_sort_keys(keyed, sort_threads);
             for (int32_t k = 0; k < count; k++) perm[begin + k] = keyed[k].second;
             const int32_t mid = count / 2;
             int32_t l, r;
@@ -315,12 +359,13 @@ void build_tree(const int32_t* edges, int32_t E, const double* h_xyz, double eps
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     int32_t split = 0;
     while ((1u << split) < std::min(hw, 16u) && ((int64_t)E >> split) > 4 * (int64_t)leaf + 4096) split++;
-    Builder top{tr.C, tr.T, tr.m, leaf, tr.perm.data(), {}, {}, {}, split > 0 ? split : -1, {}};
+    Builder top{tr.C, tr.T, tr.m, leaf, tr.perm.data(), {}, {}, {}, 1, split > 0 ? split : -1, {}};
+    top.sort_threads = (int)std::min(hw, 16u);
     top.rec(0, E);
     std::vector<Builder> sub;
     sub.reserve(top.tasks.size());
     for (size_t i = 0; i < top.tasks.size(); i++)
-        sub.push_back(Builder{tr.C, tr.T, tr.m, leaf, tr.perm.data(), {}, {}, {}, -1, {}});
+        sub.push_back(Builder{tr.C, tr.T, tr.m, leaf, tr.perm.data(), {}, {}, {}, 1, -1, {}});
     {
         // a failure inside a worker (allocation) is carried back to this thread
         std::vector<char> failed(top.tasks.size(), 0);
