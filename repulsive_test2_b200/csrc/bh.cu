@@ -519,8 +519,11 @@ struct BctRec {
         return I == J || e[2 * I] == e[2 * J] || e[2 * I] == e[2 * J + 1] || e[2 * I + 1] == e[2 * J] ||
                e[2 * I + 1] == e[2 * J + 1];
     }
-    // no edge of t shares a vertex with an edge of s (blocks_all_disjoint)
-    bool disjoint(const Node& t, const Node& s) const {
+    // no edge of t shares a vertex with an edge of s (blocks_all_disjoint); the
+    // relation is symmetric, so the smaller node's edges are looked up in the other
+    bool disjoint(const Node& t0, const Node& s0) const {
+        const Node& t = t0.count <= s0.count ? t0 : s0;
+        const Node& s = t0.count <= s0.count ? s0 : t0;
         for (int32_t k = t.begin; k < t.begin + t.count; k++) {
             const int32_t I = tr.perm[k];
             for (int q = 0; q < 2; q++) {
