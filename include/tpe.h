@@ -293,6 +293,24 @@ int32_t tpe_bct_matvec(tpe_ctx* ctx, const double* xyz, int32_t kind, const doub
                        int32_t ncols, double epsilon, double theta, double theta_t,
                        int32_t leaf_size, double* phi, int64_t* stats);
 
+/* One coarsening step of the stage-2 multigrid hierarchy (build_coarse_level,
+ * oracle/tpe_stage2_oracle.py:816-937), on the host (no device, no context):
+ * anchors (degree != 2, pinned), alternate coloring of the chains and cycles,
+ * the black vertices as the coarse level, a prolongation from the first two
+ * black neighbours (weights 1/2, or 1 from a single one), coarse edges along
+ * the fine paths with their original edges. Inputs: the level's V vertices, E
+ * edges, orig[V] (original vertex of each), each edge's original fine edges
+ * (path_edges with offsets path_off[E + 1]) and the pinned original vertices.
+ * Outputs, caller-allocated (at most V coarse vertices, E coarse edges and
+ * path_off[E] path entries): black[Vc], the prolongation p_idx[2V] / p_w[2V]
+ * (-1 where a slot is empty), cedges[2 Ec], cpath_off[Ec + 1], cpath_edges.
+ * *Vc = 0 where the oracle stops (no coarser level). */
+int32_t tpe_mg_coarsen(int32_t V, const int32_t* edges, int32_t E, const int32_t* orig,
+                       const int32_t* path_off, const int32_t* path_edges, const int32_t* pinned,
+                       int32_t npinned, int32_t min_vertices, int32_t* black, int32_t* p_idx,
+                       double* p_w, int32_t* cedges, int32_t* cpath_off, int32_t* cpath_edges,
+                       int32_t* Vc, int32_t* Ec);
+
 /* Energies of `ncurves` curves that share this context's topology (e.g. the K
  * tau-trial candidates of one line search) in one launch: xyz is
  * ncurves x V x 3, energies[ncurves]. */

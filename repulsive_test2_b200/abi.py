@@ -157,6 +157,8 @@ SIGNATURES = {
     "tpe_energy_batch": (C.c_int32, [vp, dp, C.c_int32, C.POINTER(tpe_params), C.c_int32, dp]),
     "tpe_bct_matvec": (C.c_int32, [vp, dp, C.c_int32, dp, C.c_int32, C.c_double, C.c_double, C.c_double,
                                    C.c_int32, dp, C.POINTER(C.c_int64)]),
+    "tpe_mg_coarsen": (C.c_int32, [C.c_int32, ip, C.c_int32, ip, ip, ip, ip, C.c_int32, C.c_int32, ip, ip, dp,
+                                   ip, ip, ip, ip, ip]),
     "tpe_edge_tree": (C.c_int32, [dp, C.c_int32, ip, C.c_int32, C.c_double, C.c_int32, C.c_int32, dp, ip, ip,
                                   ip]),
     "tpe_energy_bh": (C.c_int32, [vp, dp, C.POINTER(tpe_params), C.c_double, C.c_double, C.c_int32, dp,

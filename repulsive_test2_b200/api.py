@@ -251,6 +251,57 @@ def bctApplyB(vertices, edges, u, kind="high", epsilon=1e-10, theta=0.5, leafSiz
     return out, stats
 
 
+def mgHierarchy(vertices, edges, pinned=(), maxLevels=16, minVertices=8):
+    """The stage-2 multigrid's level hierarchy (build_hierarchy / build_coarse_level,
+    oracle/tpe_stage2_oracle.py:816-955), coarsened on the host by tpe_mg_coarsen: a list of
+    levels, each {"vertices", "edges", "orig_vertices", "edge_paths"} and, below the finest,
+    "P_to_fine" (the dense prolongation to the next finer level). pinned lists original
+    vertex indices (the point constraints)."""
+    lib = abi.load_library()
+    v0 = _v(vertices)
+    e0 = np.ascontiguousarray(np.asarray(edges, dtype=np.int32).reshape(-1, 2))
+    pin = np.ascontiguousarray(np.asarray(sorted(set(int(p) for p in pinned)), dtype=np.int32))
+    levels = [{"vertices": v0.copy(), "edges": e0.copy(), "orig_vertices": list(range(len(v0))),
+               "edge_paths": [[i] for i in range(len(e0))]}]
+    while len(levels) < maxLevels:
+        L = levels[-1]
+        V, E = len(L["vertices"]), len(L["edges"])
+        orig = np.ascontiguousarray(np.asarray(L["orig_vertices"], dtype=np.int32))
+        off = np.ascontiguousarray(np.cumsum([0] + [len(p) for p in L["edge_paths"]]).astype(np.int32))
+        pe = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.int32) for p in L["edge_paths"]])
+                                  if E else np.zeros(1, dtype=np.int32))
+        le = np.ascontiguousarray(L["edges"], dtype=np.int32)
+        black = np.zeros(max(V, 1), dtype=np.int32)
+        p_idx = np.zeros(max(2 * V, 1), dtype=np.int32)
+        p_w = np.zeros(max(2 * V, 1))
+        ce = np.zeros(max(2 * E, 2), dtype=np.int32)
+        coff = np.zeros(E + 2, dtype=np.int32)
+        cpe = np.zeros(max(int(off[-1]), 1), dtype=np.int32)
+        vc, ec = C.c_int32(0), C.c_int32(0)
+        rc = lib.tpe_mg_coarsen(V, le.ctypes.data_as(abi.ip), E, orig.ctypes.data_as(abi.ip),
+                                off.ctypes.data_as(abi.ip), pe.ctypes.data_as(abi.ip),
+                                pin.ctypes.data_as(abi.ip), len(pin), int(minVertices),
+                                black.ctypes.data_as(abi.ip), p_idx.ctypes.data_as(abi.ip), _dp(p_w),
+                                ce.ctypes.data_as(abi.ip), coff.ctypes.data_as(abi.ip),
+                                cpe.ctypes.data_as(abi.ip), C.byref(vc), C.byref(ec))
+        if rc != abi.TPE_OK:
+            raise TpeError(f"tpe_mg_coarsen failed with status {rc}")
+        if vc.value == 0:
+            break
+        nc, nec = vc.value, ec.value
+        P = np.zeros((V, nc))
+        for i in range(V):
+            for s in range(2):
+                if p_idx[2 * i + s] >= 0:
+                    P[i, p_idx[2 * i + s]] = p_w[2 * i + s]
+        blk = black[:nc]
+        levels.append({"vertices": L["vertices"][blk].copy(), "edges": ce[:2 * nec].reshape(-1, 2).copy(),
+                       "orig_vertices": [L["orig_vertices"][i] for i in blk],
+                       "edge_paths": [cpe[coff[j]:coff[j + 1]].tolist() for j in range(nec)],
+                       "P_to_fine": P})
+    return levels
+
+
 # ---- innerProduct.ts --------------------------------------------------------------
 
 def _assemble(vertices, edges, which, alpha, beta, epsilon):

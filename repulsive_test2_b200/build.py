@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libtpe.so")
 OBJ = os.path.join(HERE, "_build")
 
-SOURCES = ["api.cu", "pair_kernels.cu", "assembly.cu", "dense.cu", "constraints.cu", "noalloc.cu", "pair_mixed.cu", "tc_gemm.cu", "ozaki.cu", "mixed.cu", "schur.cu", "batch.cu", "bh.cu"]
+SOURCES = ["api.cu", "pair_kernels.cu", "assembly.cu", "dense.cu", "constraints.cu", "noalloc.cu", "pair_mixed.cu", "tc_gemm.cu", "ozaki.cu", "mixed.cu", "schur.cu", "batch.cu", "bh.cu", "mg.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

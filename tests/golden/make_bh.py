@@ -22,6 +22,9 @@ phi, the dense product exact_edge_kernel_sym @ psi and the block counts
 (leaves, admissible blocks, direct blocks, direct pairs). bh_trees.npz holds the
 oracle's trees (build_edge_bvh) node by node: center, mean tangent, mass, radii,
 children and edge lists, for a trefoil, the loop network and a 20000-edge walk.
+mg_levels.npz holds the oracle's multigrid hierarchies (build_hierarchy): every
+level's edges, original vertices, edge paths and prolongation, for a trefoil, the
+loop network with 4 pins and a random walk with 3 pins.
 """
 from __future__ import annotations
 
@@ -132,6 +135,31 @@ def main():
         trees[name + "/idx"] = np.concatenate([nd.indices for nd in nodes]).astype(np.int32)
         print(f"tree {name}: {len(nodes)} nodes")
     np.savez_compressed(os.path.join(HERE, "bh_trees.npz"), **trees)
+
+    # the multigrid hierarchy (build_hierarchy / build_coarse_level)
+    mg = {}
+    vw, ew = fixtures.random_walk_knot(512, seed=17)
+    pins_net = [int(p) for p in fixtures.seeded_pins(len(vnet), 4, seed=2)]
+    for name, v, e, pins in (("trefoil120", v120, e120, []), ("network_pins4", vnet, enet, pins_net),
+                             ("walk512_pins3", vw, ew, [5, 200, 401])):
+        v = np.asarray(v, dtype=np.float64)
+        e = np.asarray(e, dtype=np.int64)
+        spec = O.ConstraintSpec(points=tuple((p, tuple(v[p])) for p in pins))
+        levels = O.build_hierarchy(v, e, spec)
+        mg[name + "/vertices"] = v
+        mg[name + "/edges"] = e.astype(np.int32)
+        mg[name + "/pins"] = np.asarray(pins, dtype=np.int32)
+        mg[name + "/nlevels"] = np.array([len(levels)])
+        for li, L in enumerate(levels):
+            key = f"{name}/L{li}"
+            mg[key + "/edges"] = np.asarray(L.edges, dtype=np.int32)
+            mg[key + "/orig"] = np.asarray(L.orig_vertices, dtype=np.int32)
+            mg[key + "/path_off"] = np.cumsum([0] + [len(p) for p in L.edge_paths]).astype(np.int32)
+            mg[key + "/path_edges"] = np.concatenate([np.asarray(p, dtype=np.int32) for p in L.edge_paths])
+            if L.P_to_fine is not None:
+                mg[key + "/P"] = L.P_to_fine
+        print(f"hierarchy {name}: levels {[len(L.vertices) for L in levels]}")
+    np.savez_compressed(os.path.join(HERE, "mg_levels.npz"), **mg)
 
     # the Sobolev operators through the products (bct_apply_B_scalar)
     u = np.sin(np.arange(120) * 0.7)

@@ -115,3 +115,25 @@ def test_edge_tree_is_the_oracle_tree(name):
             stack.append((l, links[theirs][0]))
             stack.append((r, links[theirs][1]))
     assert seen == len(f_o)
+
+
+MG = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                "golden", "mg_levels.npz")
+
+
+@pytest.mark.parametrize("name", ["trefoil120", "network_pins4", "walk512_pins3"])
+def test_mg_hierarchy_is_the_oracle_hierarchy(name):
+    """api.mgHierarchy (tpe_mg_coarsen per level) against the oracle's build_hierarchy: the
+    same number of levels and, level by level, the same coarse edges, original vertices,
+    original edge paths and prolongation to the finer level."""
+    z = np.load(MG)
+    levels = T.mgHierarchy(z[name + "/vertices"], z[name + "/edges"], pinned=z[name + "/pins"])
+    assert len(levels) == int(z[name + "/nlevels"][0])
+    for li, L in enumerate(levels):
+        key = f"{name}/L{li}"
+        np.testing.assert_array_equal(L["edges"], z[key + "/edges"])
+        np.testing.assert_array_equal(L["orig_vertices"], z[key + "/orig"])
+        off, pe = z[key + "/path_off"], z[key + "/path_edges"]
+        assert [list(p) for p in L["edge_paths"]] == [list(pe[off[j]:off[j + 1]]) for j in range(len(off) - 1)]
+        if li > 0:
+            np.testing.assert_array_equal(L["P_to_fine"], z[key + "/P"])
